@@ -1,0 +1,245 @@
+/*
+ * jfcut.h — C ABI of the B200 grid graph-cut solver (libjfcut.so).
+ *
+ * The surface keeps JF-Cut's graph-cut operator: build a 4-/6-connected grid
+ * graph from an image / video / volume plus seed strokes, compute the exact
+ * max-flow, read back the min-cut labels.  In the reference this surface is
+ * the QGCWidget class (src/QVisualizer/Graph Cut/QGCWidget.h:160-243) driving
+ * OpenCL kernels; there is no FFI there, so every entry point below names the
+ * reference method or file format it replaces.
+ *
+ * Conventions
+ *  - Every function returns an int status (JFC_OK = 0) unless stated; no C++
+ *    exception crosses this boundary.  Errors replace the reference's
+ *    QError(level, code) (infrastructures/QError.h:37-73).
+ *  - Host buffers are owned by the caller and are only read/written during the
+ *    call.  Device buffers (the *_device variants) are caller-owned device
+ *    pointers on the context's device.
+ *  - Node order is x-fastest: index = x + W*(y + H*z).
+ *  - Residual / capacity arrays follow the reference channel order:
+ *      2D: [0]=+x [1]=+y [2]=-y [3]=-x      (cl_ushort2 c1=(+x,+y), c2=(-y,-x);
+ *                                            QGCWidget.cpp:2479-2482)
+ *      3D: [0]=+x [1]=+y [2]=+z [3]=-z [4]=-y [5]=-x
+ *                                           (cl_uchar4 c1=(+x,+y,+z), c2=(-z,-y,-x);
+ *                                            QGCWidget.cpp:2503-2508)
+ *    ncap[k][i] is the capacity of the arc leaving node i in direction k.
+ *    Arcs that would leave the grid must be 0.
+ *  - Terminal links use the reference's net-excess form
+ *    (graphcut_compute_excessflow.cl:39-44): excess[i] = cs[i] - ct[i].
+ *    flow_offset = sum_i min(cs[i], ct[i]) (0 for graphs given as net excess).
+ *    Max-flow values are int64.
+ *  - Labels: 1 = source side (the reference's cut.object = CHAR_MAX), 0 = sink
+ *    side.  The source side is the canonical (minimal) one: the nodes reachable
+ *    from excess in the final residual graph (graphcut_compute_cut.cl:36-125).
+ */
+#ifndef JFCUT_H
+#define JFCUT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (replace QError levels, QGCWidget.cpp:2017, 3112-3116) ---- */
+enum {
+  JFC_OK = 0,
+  JFC_ERR_INVALID_ARG = 1,   /* bad size, null pointer, unsupported connectivity */
+  JFC_ERR_NO_SEEDS = 2,      /* "no labels" (QGCWidget.cpp:2017, 3112) */
+  JFC_ERR_OOM = 3,           /* device allocation failed / over HBM budget */
+  JFC_ERR_NOT_CONVERGED = 4, /* iteration budget hit; never silent (QGCWidget.cpp:2413) */
+  JFC_ERR_CUDA = 5,          /* CUDA runtime error */
+  JFC_ERR_NO_DEVICE = 6,     /* no CUDA device / extension cannot run here */
+  JFC_ERR_STATE = 7,         /* call out of order (e.g. labels before solve) */
+  JFC_ERR_CANCELLED = 8,     /* server request cancelled */
+  JFC_ERR_BUSY = 9           /* server queue full / request not finished */
+};
+
+/* Pixel formats of jfc_graph_build_from_image (the reference reads a float
+ * volume plus an RGBA8 feature image, QGCWidget.cpp:1309-1368). */
+enum {
+  JFC_PIX_GRAY8 = 0,   /* uint8, 1 channel */
+  JFC_PIX_RGB8 = 1,    /* uint8, 3 channels interleaved */
+  JFC_PIX_I16 = 2      /* int16, 1 channel (CT/MR style volumes) */
+};
+
+/* Seed byte values (cl_cut.foreground / background, QGCSetting.h:46-52). */
+enum { JFC_SEED_NONE = 0, JFC_SEED_FG = 1, JFC_SEED_BG = 2 };
+
+/* Solver schedule.  Replaces the Convergence panel (countIterations,
+ * cutIterations, totalIterations: QGCPanel.ui:1494-1658) and the tile
+ * constants (QGCSetting.cpp:28-29).  Zero fields take defaults. */
+typedef struct jfc_params {
+  int tile_rows;         /* 2D warp-tile height: 8 or 16 (default 16); 3D uses 32x4x4 */
+  int local_iters;       /* push/relabel rounds per tile visit (default 16) */
+  int relabel_interval;  /* parity sweeps between global relabels (default 8) */
+  int max_sweeps;        /* budget of sweeps -> JFC_ERR_NOT_CONVERGED (default 1<<20) */
+  int max_bfs_passes;    /* budget of tile passes per BFS (default 1<<20) */
+  int use_graph;         /* 1: capture the solve loop in a CUDA graph (default 1) */
+  int verbose;           /* 1: one JSON line per solve on stderr */
+} jfc_params;
+
+/* Capacity model (replaces computeCapacity / kmeans / computeExcessFlowLazy,
+ * QGCWidget.cpp:1997-2107, 3182-3235).  All weights are integer by
+ * construction (host-built int32 lookup tables), so device and CPU builds are
+ * bit-identical. */
+typedef struct jfc_model {
+  int lambda_n;          /* n-link scale: w = round(lambda_n*exp(-D/(2 sigma^2))) (default 100) */
+  int z_weight_pct;      /* 3D z-direction n-link scale in percent (default 100; video 50) */
+  int lambda_t;          /* t-link scale: round(lambda_t * -ln p) (default 10) */
+  int k_fg;              /* k-means clusters for the object model (default 5) */
+  int k_bg;              /* k-means clusters for the background model (default 5) */
+  int seed_cap;          /* hard seed t-link capacity (default 1000000) */
+  int kmeans_iters;      /* k-means iteration cap (default 32, QGCWidget.cpp:2073) */
+} jfc_model;
+
+/* Per-solve statistics (the reference prints these as "> GPU TIME" / "> DATA",
+ * QGCWidget.cpp:2522-2524). */
+typedef struct jfc_stats {
+  int status;
+  int sweeps;             /* parity sweeps (one even + one odd = one iteration) */
+  int global_relabels;
+  int bfs_passes;         /* tile passes summed over all BFS runs */
+  long long tile_visits;  /* push-relabel tile visits */
+  long long flow;         /* max-flow value (int64) */
+  long long source_nodes; /* nodes on the source side */
+  double ms_total, ms_build, ms_push_relabel, ms_global_relabel, ms_cut;
+} jfc_stats;
+
+typedef struct jfc_ctx jfc_ctx;
+typedef struct jfc_graph jfc_graph;
+typedef struct jfc_batch jfc_batch;
+typedef struct jfc_server jfc_server;
+
+/* ---- context (replaces QGCWidget::initContext / initOpenCL, QGCWidget.cpp:686-813) ---- */
+int  jfc_create(int device, const jfc_params* params, jfc_ctx** out);
+void jfc_destroy(jfc_ctx* ctx);
+int  jfc_set_params(jfc_ctx* ctx, const jfc_params* params);
+int  jfc_get_params(jfc_ctx* ctx, jfc_params* out);
+void jfc_default_params(jfc_params* out);
+void jfc_default_model(jfc_model* out);
+const char* jfc_strerror(int status);
+/* Detail of the last error raised on the calling thread (the reference's
+ * QError message / cl::Error string, QGCWidget.cpp:2533-2557). */
+const char* jfc_last_error(void);
+/* Run the context's work on a caller-owned CUDA stream (a cudaStream_t passed
+ * as void*; NULL restores the context's own stream).  Lets a caller bracket
+ * the library's kernels with its own CUDA events (the reference times every
+ * phase with OpenCL profiling events, utilities/QUtilityCL.cpp:341-354). */
+int  jfc_set_stream(jfc_ctx* ctx, void* stream);
+/* Number of CUDA kernels this library has launched in this process. */
+unsigned long long jfc_kernel_launches(void);
+
+/* ---- graph (replaces initConfigurations' buffer sizing, QGCWidget.cpp:815-887) ---- */
+/* dims = 2 (conn 4, d = 1) or 3 (conn 6). */
+int  jfc_graph_create_grid(jfc_ctx* ctx, int dims, int w, int h, int d, int conn, jfc_graph** out);
+void jfc_graph_destroy(jfc_graph* g);
+/* Bytes of device memory a grid of this shape holds (HBM-budget admission). */
+size_t jfc_graph_bytes(int dims, int w, int h, int d);
+
+/* Build n-links and t-links from an image and seeds (host buffers).
+ * Replaces slotModelClicked -> computeCapacity + kmeans + computeExcessFlowLazy
+ * (QGCWidget.cpp:2560-2606).  Returns JFC_ERR_NO_SEEDS when either class has
+ * no seed.  img: w*h*d pixels in pixfmt; seeds: w*h*d bytes (JFC_SEED_*). */
+int jfc_graph_build_from_image(jfc_graph* g, const void* img, int pixfmt,
+                               const uint8_t* seeds, const jfc_model* model);
+/* Same, with img and seeds already in device memory. */
+int jfc_graph_build_from_device(jfc_graph* g, const void* d_img, int pixfmt,
+                                const uint8_t* d_seeds, const jfc_model* model);
+
+/* Load an explicit graph (replaces slotLoadGraphClicked's .ef/.c1/.c2 load,
+ * QGCWidget.cpp:2631-2736).  excess: n int32; ncap: conn pointers to n int32. */
+int jfc_graph_set(jfc_graph* g, const int32_t* excess, const int32_t* const* ncap,
+                  int64_t flow_offset);
+int jfc_graph_set_device(jfc_graph* g, const int32_t* d_excess,
+                         const int32_t* const* d_ncap, int64_t flow_offset);
+/* Read the current residual state (net excess, residual arcs, heights).
+ * Any pointer may be NULL.  Used for certificates and .ef/.c1/.c2 export. */
+int jfc_graph_get_state(jfc_graph* g, int32_t* excess, int32_t* const* ncap, int32_t* height);
+
+/* Solve to the exact max-flow / min-cut.  Replaces slotCutClicked's hot loop
+ * (QGCWidget.cpp:2364-2558): global relabel, push/relabel sweeps, device-side
+ * convergence, final residual BFS.  Warm: a second call after
+ * jfc_edit_tlinks continues from the resident residual graph. */
+int jfc_solve(jfc_graph* g, jfc_stats* stats);
+int jfc_get_flow(jfc_graph* g, int64_t* flow);
+/* Labels (1 = source side).  Replaces the cut read-back (QGCWidget.cpp:2454,
+ * slotSaveCutClicked 2990-2996). */
+int jfc_read_labels(jfc_graph* g, uint8_t* out);
+int jfc_read_labels_device(jfc_graph* g, uint8_t* d_out);
+
+/* Warm-start stroke edit: node idx[j] gets cs += dcs[j], ct += dct[j].
+ * (New in this build: the reference re-models from scratch on every stroke,
+ * QGCWidget.cpp:2560.)  The residual graph and heights stay resident. */
+int jfc_edit_tlinks(jfc_graph* g, const uint32_t* idx, const int32_t* dcs,
+                    const int32_t* dct, size_t n);
+/* Warm-start stroke edit on a graph built from an image: node idx[j] becomes
+ * seed new_seed[j] (JFC_SEED_*) with the colour model kept fixed; the t-link
+ * change is applied to the resident residual graph (the reference re-runs
+ * slotModelClicked, QGCWidget.cpp:2560-2606, after every brush stroke,
+ * QGCWidget.cpp:2243-2287).  Duplicate indices: the last one wins. */
+int jfc_graph_edit_seeds(jfc_graph* g, const uint32_t* idx, const uint8_t* new_seed, size_t n);
+
+/* ---- batched solver: many independent grids in one persistent launch per
+ * phase, fed by a device work queue (no reference counterpart; the reference
+ * solves one volume at a time, QGCWidget.cpp:2364). ---- */
+int  jfc_batch_create(jfc_ctx* ctx, jfc_batch** out);
+void jfc_batch_destroy(jfc_batch* b);
+int  jfc_batch_add(jfc_batch* b, jfc_graph* g);     /* graph must be built/set */
+int  jfc_batch_clear(jfc_batch* b);
+int  jfc_batch_size(jfc_batch* b);
+/* Solve every graph of the batch; stats may be NULL or an array of the
+ * batch's size.  Returns the first non-OK per-graph status. */
+int  jfc_batch_solve(jfc_batch* b, jfc_stats* stats);
+/* Pick tile_rows / local_iters / relabel_interval for this batch by timing
+ * candidates on a copy of the batch's graphs (state is restored). */
+int  jfc_batch_autotune(jfc_batch* b, jfc_params* chosen);
+
+/* ---- serving: continuous batching with HBM-budget admission and warm
+ * stroke edits (no reference counterpart). ---- */
+typedef struct jfc_request_info {
+  int status;
+  int64_t flow;
+  double ms_queue, ms_solve, ms_total;   /* latency split */
+  int warm;                              /* 1 if re-solved from resident state */
+} jfc_request_info;
+
+int  jfc_server_create(jfc_ctx* ctx, size_t hbm_budget_bytes, int max_slots, jfc_server** out);
+void jfc_server_destroy(jfc_server* s);
+/* Submit a new session from host image + seeds; returns a session id >= 0 in *sid. */
+int  jfc_server_submit(jfc_server* s, int dims, int w, int h, int d, const void* img, int pixfmt,
+                       const uint8_t* seeds, const jfc_model* model, int* sid);
+/* Queue a stroke edit (re-seed nodes) for an existing session; re-solved warm
+ * from the session's resident residual graph. */
+int  jfc_server_edit(jfc_server* s, int sid, const uint32_t* idx, const uint8_t* new_seed, size_t n);
+/* Block until the session's latest request is finished (timeout_ms < 0: forever). */
+int  jfc_server_wait(jfc_server* s, int sid, int timeout_ms, jfc_request_info* info);
+int  jfc_server_read_labels(jfc_server* s, int sid, uint8_t* out);
+int  jfc_server_close(jfc_server* s, int sid);      /* frees the session's device state */
+int  jfc_server_cancel(jfc_server* s, int sid);
+
+/* ---- synthetic inputs (seeded, deterministic, integer arithmetic) used by the
+ * tests and the benchmark in place of the reference's image files ---- */
+/* 2D gray: blurred ellipse (fg 170 / bg 80) + N(0,sigma) noise, 1-px strokes. */
+int jfc_synth_gray_ellipse(int w, int h, uint64_t seed, int noise_sigma,
+                           uint8_t* img, uint8_t* seeds);
+/* 2D RGB: n_ellipses random overlapping ellipses, region means U(0,255)^3,
+ * N(0,noise_sigma) noise, random strokes covering stroke_permille/1000 of pixels. */
+int jfc_synth_rgb_ellipses(int w, int h, uint64_t seed, int n_ellipses, int noise_sigma,
+                           int stroke_permille_x10, uint8_t* img, uint8_t* seeds);
+/* 3D RGB video: ellipse moving 4 px/frame over value-noise texture; strokes on
+ * the first and last frame. */
+int jfc_synth_rgb_video(int w, int h, int frames, uint64_t seed, uint8_t* img, uint8_t* seeds);
+/* 3D int16 volume: sphere-and-tube phantom + N(0,noise_sigma) noise; seed blobs. */
+int jfc_synth_i16_phantom(int w, int h, int d, uint64_t seed, int noise_sigma,
+                          int16_t* img, uint8_t* seeds);
+/* Random brush stroke: a seeded walk over up to n distinct nodes, all given
+ * seed value `label`; *n_out receives the number of nodes written. */
+int jfc_synth_stroke(int dims, int w, int h, int d, uint64_t seed, size_t n, uint8_t label,
+                     uint32_t* idx, uint8_t* new_seed, size_t* n_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JFCUT_H */

@@ -1,0 +1,185 @@
+// batch.cpp — batched solver: many independent grids of uneven sizes share
+// every launch.
+//
+// No reference counterpart: JF-Cut solves one volume at a time
+// (QGCWidget::slotCutClicked, QGCWidget.cpp:2364).  The per-grid arithmetic is
+// unchanged; what changes is that all grids' tiles form one tile set, so every
+// sweep / BFS pass is one persistent launch whose warps pull tiles of any grid
+// from the device work queue, and the host loop runs once for the whole batch
+// (converged grids simply stop producing flagged tiles).  The autotuner times
+// candidate schedules (tile height, rounds per visit, relabel interval) on the
+// batch itself and restores the graphs' state after each trial.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+#include "engine.h"
+
+struct jfc_batch {
+  jfc_ctx* ctx = nullptr;
+  std::vector<jfc_graph*> graphs;
+  TileSet ts[2];          // [0] 2D grids, [1] 3D grids
+  int shape[2] = {-1, -1};
+  bool dirty = true;
+};
+
+namespace {
+
+int rebuild(jfc_batch* b) {
+  const int tr = b->ctx->params.tile_rows;
+  for (int k = 0; k < 2; ++k) {
+    const int dims = k ? 3 : 2;
+    const int code = shape_code(dims, tr);
+    if (!b->dirty && b->shape[k] == code) continue;
+    std::vector<GridDev> v;
+    for (jfc_graph* g : b->graphs)
+      if (g->dims == dims) v.push_back(g->g);
+    tileset_free(b->ts[k]);
+    b->shape[k] = -1;
+    if (v.empty()) continue;
+    int rc = tileset_build(b->ts[k], dims, tr, v);
+    if (rc) return rc;
+    b->shape[k] = code;
+  }
+  b->dirty = false;
+  return JFC_OK;
+}
+
+// Device snapshot of every graph's e and residual planes (autotuner).
+struct Snapshot {
+  std::vector<void*> bufs;
+  ~Snapshot() { for (void* p : bufs) cudaFree(p); }
+};
+
+int snapshot(jfc_batch* b, Snapshot& s, bool restore) {
+  cudaStream_t st = b->ctx->stream;
+  for (size_t i = 0; i < b->graphs.size(); ++i) {
+    jfc_graph* g = b->graphs[i];
+    const size_t bytes = (size_t)g->g.plane * 4 * (1 + g->conn);
+    if (!restore) {
+      void* p = nullptr;
+      JFC_CUDA(cudaMalloc(&p, bytes));
+      s.bufs.push_back(p);
+    }
+    char* p = (char*)s.bufs[i];
+    const size_t pb = (size_t)g->g.plane * 4;
+    int* planes[7] = {g->g.e, g->g.r[0], g->g.r[1], g->g.r[2], g->g.r[3], g->g.r[4], g->g.r[5]};
+    for (int k = 0; k < 1 + g->conn; ++k) {
+      if (restore) JFC_CUDA(cudaMemcpyAsync(planes[k], p + k * pb, pb, cudaMemcpyDeviceToDevice, st));
+      else JFC_CUDA(cudaMemcpyAsync(p + k * pb, planes[k], pb, cudaMemcpyDeviceToDevice, st));
+    }
+  }
+  JFC_CUDA(cudaStreamSynchronize(st));
+  return JFC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int jfc_batch_create(jfc_ctx* ctx, jfc_batch** out) {
+  if (!ctx || !out) return set_error(JFC_ERR_INVALID_ARG, "null argument");
+  jfc_batch* b = new jfc_batch();
+  b->ctx = ctx;
+  *out = b;
+  return JFC_OK;
+}
+
+void jfc_batch_destroy(jfc_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->ctx->device);
+  tileset_free(b->ts[0]);
+  tileset_free(b->ts[1]);
+  delete b;
+}
+
+int jfc_batch_add(jfc_batch* b, jfc_graph* g) {
+  if (!b || !g) return set_error(JFC_ERR_INVALID_ARG, "null argument");
+  if (g->ctx != b->ctx) return set_error(JFC_ERR_INVALID_ARG, "graph belongs to another context");
+  if (g->state == 0) return set_error(JFC_ERR_STATE, "graph is empty");
+  b->graphs.push_back(g);
+  b->dirty = true;
+  return JFC_OK;
+}
+
+int jfc_batch_clear(jfc_batch* b) {
+  if (!b) return set_error(JFC_ERR_INVALID_ARG, "null batch");
+  b->graphs.clear();
+  b->dirty = true;
+  return JFC_OK;
+}
+
+int jfc_batch_size(jfc_batch* b) { return b ? (int)b->graphs.size() : 0; }
+
+int jfc_batch_solve(jfc_batch* b, jfc_stats* stats) {
+  if (!b) return set_error(JFC_ERR_INVALID_ARG, "null batch");
+  JFC_CUDA(cudaSetDevice(b->ctx->device));
+  for (jfc_graph* g : b->graphs)
+    if (g->state == 0) return set_error(JFC_ERR_STATE, "graph is empty");
+  int rc = rebuild(b);
+  if (rc) return rc;
+  int first_bad = JFC_OK;
+  for (int k = 0; k < 2; ++k) {
+    if (b->shape[k] < 0) continue;
+    const int dims = k ? 3 : 2;
+    std::vector<GridResult> res;
+    jfc_stats st;
+    rc = engine_solve(b->ctx, b->ts[k], b->ctx->params, res, st);
+    if (rc && rc != JFC_ERR_NOT_CONVERGED) return rc;
+    int gi = 0;
+    for (size_t i = 0; i < b->graphs.size(); ++i) {
+      jfc_graph* g = b->graphs[i];
+      if (g->dims != dims) continue;
+      const GridResult& r = res[gi++];
+      g->flow = g->sink_total + r.neg_sum;
+      g->source_nodes = r.labels;
+      g->state = r.status ? 1 : 2;
+      jfc_stats gs = st;
+      gs.status = r.status;
+      gs.flow = g->flow;
+      gs.source_nodes = g->source_nodes;
+      g->last = gs;
+      if (stats) stats[i] = gs;
+      if (r.status && !first_bad) first_bad = r.status;
+    }
+  }
+  return first_bad;
+}
+
+int jfc_batch_autotune(jfc_batch* b, jfc_params* chosen) {
+  if (!b) return set_error(JFC_ERR_INVALID_ARG, "null batch");
+  if (b->graphs.empty()) return set_error(JFC_ERR_STATE, "empty batch");
+  JFC_CUDA(cudaSetDevice(b->ctx->device));
+  Snapshot snap;
+  int rc = snapshot(b, snap, false);
+  if (rc) return rc;
+  const jfc_params base = b->ctx->params;
+  jfc_params best = base;
+  double best_ms = 1e30;
+  const int rows[] = {8, 16};
+  const int iters[] = {8, 16, 32};
+  const int intervals[] = {2, 4, 8, 16};
+  for (int tr : rows)
+    for (int li : iters)
+      for (int ri : intervals) {
+        jfc_params p = base;
+        p.tile_rows = tr; p.local_iters = li; p.relabel_interval = ri;
+        b->ctx->params = p;
+        rc = snapshot(b, snap, true);
+        if (rc) { b->ctx->params = base; return rc; }
+        auto t0 = std::chrono::steady_clock::now();
+        rc = jfc_batch_solve(b, nullptr);
+        auto t1 = std::chrono::steady_clock::now();
+        if (rc) continue;
+        const double ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        if (ms < best_ms) { best_ms = ms; best = p; }
+      }
+  b->ctx->params = best;
+  rc = snapshot(b, snap, true);
+  for (jfc_graph* g : b->graphs) g->state = 1;
+  if (chosen) *chosen = best;
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,124 @@
+// jfc_internal.h — shared device/host definitions of libjfcut.
+//
+// Data layout in HBM (one grid instance):
+//   planes of int32 e (net excess), h (height), r[conn] (residual capacity of
+//   the arc leaving the node in direction k, reference channel order), plus a
+//   uint8 label plane.  Every plane is padded to pitch x Hp x Dp with
+//   pitch = roundup(W, 32) and Hp / Dp multiples of the largest tile extent, so
+//   a warp tile never needs a bounds check.  Padding nodes are inert: e = 0,
+//   r = 0, h = INF (they have no residual arc in or out).
+// Work is organised in warp tiles: 32 columns (one per lane) x TR rows (2D) or
+// 32 x TY x TZ (3D); each lane keeps its column's state in registers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/jfcut.h"
+
+#define JFC_INF (1 << 30)
+#define JFC_TW 32           // tile width = warp width
+#define JFC_PAD_Y2 16       // 2D row padding (covers tile heights 4, 8, 16)
+#define JFC_PAD_YZ3 4       // 3D y/z padding (covers 4x4, 4x2, 2x4 tiles)
+#define JFC_MAX_K 32        // k-means clusters per class
+#define JFC_TQ 65536        // t-link probability quantisation
+
+// Device-side descriptor of one grid instance.
+struct GridDev {
+  int dims, W, H, D;
+  int pitch, Hp, Dp;
+  int tiles_x, tiles_y, tiles_z;
+  int tile_base;             // global id of this grid's first tile
+  long long plane;           // pitch * Hp * Dp
+  int* e;
+  int* h;
+  int* r[6];
+  uint8_t* label;
+};
+
+// Per-launch work-queue ticket (reset by the last block of each launch).
+struct Ticket {
+  unsigned int chunk;
+  unsigned int done;
+};
+
+// Device-side counters of one solve (one per tile set).
+struct DevCounters {
+  Ticket tk;                 // work queue ticket
+  int pending[2];            // BFS: a tile was flagged for the next pass
+  int cut_bad;               // cut BFS reached a deficit node (augmenting path left)
+  int pad_;
+  unsigned long long visits; // push-relabel tile visits
+  unsigned long long bfs_visits;
+};
+
+// A set of grids tiled with one tile shape: the unit every launch works on
+// (a plain solve is a set of one grid; a batch concatenates many).
+struct TileSet {
+  int dims = 2;
+  int TR = 16, TY = 4, TZ = 4;       // tile shape (2D: 32xTR, 3D: 32xTYxTZ)
+  int ngrids = 0;
+  int ntiles = 0;
+  GridDev* d_desc = nullptr;         // [ngrids]
+  int4* d_info = nullptr;            // [ntiles] {grid, tx, ty, tz}
+  int* d_list[2] = {nullptr, nullptr};  // tile ids of parity 0 / 1
+  int nlist[2] = {0, 0};
+  uint8_t* d_flag_pr = nullptr;      // [ntiles] tile has active nodes
+  uint8_t* d_flag_bfs[2] = {nullptr, nullptr};  // [ntiles] BFS double buffer
+  int* d_grid_active = nullptr;      // [ngrids] active tiles after global relabel
+  long long* d_grid_sum = nullptr;   // [ngrids*2] sum min(e,0), source-side count
+  DevCounters* d_ctr = nullptr;
+  void* d_block = nullptr;           // single allocation backing the above
+  size_t block_bytes = 0;
+};
+
+// Counts every kernel launch of the library (engine.cpp).
+void jfc_note_launch(int n = 1);
+
+// ----------------------------------------------------------- kernel launchers
+// (kernels_pr.cu)
+cudaError_t launch_pr_sweep(const TileSet& ts, int parity, int local_iters, cudaStream_t s);
+// (kernels_bfs.cu)
+cudaError_t launch_relabel_pass(const TileSet& ts, int pass, bool first, cudaStream_t s);
+cudaError_t launch_cut_pass(const TileSet& ts, int pass, bool first, cudaStream_t s);
+cudaError_t launch_grid_sums(const TileSet& ts, cudaStream_t s);
+cudaError_t launch_clear_counters(const TileSet& ts, cudaStream_t s);
+int persistent_blocks(const void* kernel, int threads, size_t smem);
+// layout helpers (kernels_bfs.cu)
+cudaError_t launch_fix_boundary(const GridDev& g, int conn, int* d_bad, cudaStream_t s);
+cudaError_t launch_pack_labels(const GridDev& g, uint8_t* d_dense, cudaStream_t s);
+cudaError_t launch_pack_plane(const GridDev& g, const int* d_plane, int* d_dense, cudaStream_t s);
+cudaError_t launch_edit_tlinks(const GridDev& g, const uint32_t* d_idx, const int32_t* d_dcs,
+                               const int32_t* d_dct, size_t n, long long* d_dsink, cudaStream_t s);
+
+// (kernels_build.cu) capacity build
+struct BuildModelDev {
+  int pixfmt, channels;
+  int kf, kb;
+  int seed_cap;
+  int mu_f[JFC_MAX_K * 3];
+  int mu_b[JFC_MAX_K * 3];
+};
+cudaError_t launch_contrast_sum(const GridDev& g, const void* d_img, int pixfmt,
+                                unsigned long long* d_sum, cudaStream_t s);
+cudaError_t launch_seed_stats(const GridDev& g, const void* d_img, int pixfmt, const uint8_t* d_seeds,
+                              int* d_minmax /*[2][3][2]*/, unsigned long long* d_count /*[2]*/,
+                              uint32_t* d_list_f, uint32_t* d_list_b, unsigned int* d_fill /*[2]*/,
+                              bool fill, cudaStream_t s);
+cudaError_t launch_kmeans_assign(const uint32_t* d_list, unsigned int n, int channels, int k,
+                                 const int* mu, unsigned long long* d_acc /*[k*4]*/, cudaStream_t s);
+cudaError_t launch_build_graph(const GridDev& g, const void* d_img, const uint8_t* d_seeds,
+                               const BuildModelDev& m, const int* d_lut_xy, const int* d_lut_z,
+                               const int* d_lut_s, const int* d_lut_t,
+                               unsigned long long* d_sink, cudaStream_t s);
+cudaError_t launch_edit_seeds(const GridDev& g, const void* d_img, uint8_t* d_seeds,
+                              const BuildModelDev& m, const int* d_lut_s, const int* d_lut_t,
+                              const uint32_t* d_idx, const uint8_t* d_new, size_t n,
+                              long long* d_dsink, cudaStream_t s);
+
+// Pixel feature helpers shared by host and device code.
+__host__ __device__ inline int jfc_pix_channels(int pixfmt) { return pixfmt == JFC_PIX_RGB8 ? 3 : 1; }
+__host__ __device__ inline size_t jfc_pix_bytes(int pixfmt) {
+  return pixfmt == JFC_PIX_RGB8 ? 3 : (pixfmt == JFC_PIX_I16 ? 2 : 1);
+}

@@ -1,0 +1,452 @@
+"""Python host mirror of the JF-Cut graph-cut operator over libjfcut.so (C ABI).
+
+The reference's operator is the QGCWidget class (src/QVisualizer/Graph Cut/
+QGCWidget.h:160-243).  This module keeps its vocabulary: a Graph is built from
+an image plus seed strokes (slotModelClicked, QGCWidget.cpp:2560-2606) or loaded
+from excess / capacity arrays (slotLoadGraphClicked, :2631-2736), solved
+(slotCutClicked, :2364-2558) and read back as labels (cut.object) and an int64
+max-flow.  Every call goes to the CUDA library; there is no CPU fallback — if
+the library is missing or no GPU is present the call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libjfcut.so")
+
+OK, ERR_INVALID_ARG, ERR_NO_SEEDS, ERR_OOM, ERR_NOT_CONVERGED, ERR_CUDA, ERR_NO_DEVICE, ERR_STATE, \
+    ERR_CANCELLED, ERR_BUSY = range(10)
+PIX_GRAY8, PIX_RGB8, PIX_I16 = 0, 1, 2
+SEED_NONE, SEED_FG, SEED_BG = 0, 1, 2
+
+
+class JfcError(RuntimeError):
+    def __init__(self, code, where=""):
+        self.code = code
+        lib = _lib()
+        msg = lib.jfc_strerror(code).decode()
+        detail = lib.jfc_last_error().decode()
+        super().__init__("%s: %s (%s)%s" % (where, msg, detail, "" if code else ""))
+
+
+class Params(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("tile_rows", "local_iters", "relabel_interval", "max_sweeps",
+                                             "max_bfs_passes", "use_graph", "verbose")]
+
+
+class Model(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("lambda_n", "z_weight_pct", "lambda_t", "k_fg", "k_bg",
+                                             "seed_cap", "kmeans_iters")]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("sweeps", ctypes.c_int), ("global_relabels", ctypes.c_int),
+                ("bfs_passes", ctypes.c_int), ("tile_visits", ctypes.c_longlong), ("flow", ctypes.c_longlong),
+                ("source_nodes", ctypes.c_longlong), ("ms_total", ctypes.c_double), ("ms_build", ctypes.c_double),
+                ("ms_push_relabel", ctypes.c_double), ("ms_global_relabel", ctypes.c_double),
+                ("ms_cut", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("flow", ctypes.c_int64), ("ms_queue", ctypes.c_double),
+                ("ms_solve", ctypes.c_double), ("ms_total", ctypes.c_double), ("warm", ctypes.c_int)]
+
+
+_LIB = None
+VP = ctypes.c_void_p
+I32P = ctypes.POINTER(ctypes.c_int32)
+U8P = ctypes.POINTER(ctypes.c_uint8)
+U32P = ctypes.POINTER(ctypes.c_uint32)
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libjfcut.so is not built (run `make -C jf-cut_b200`)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.jfc_strerror.restype = ctypes.c_char_p
+        L.jfc_last_error.restype = ctypes.c_char_p
+        L.jfc_graph_bytes.restype = ctypes.c_size_t
+        L.jfc_graph_bytes.argtypes = [ctypes.c_int] * 4
+        L.jfc_create.argtypes = [ctypes.c_int, ctypes.POINTER(Params), ctypes.POINTER(VP)]
+        L.jfc_destroy.argtypes = [VP]
+        L.jfc_destroy.restype = None
+        L.jfc_set_params.argtypes = [VP, ctypes.POINTER(Params)]
+        L.jfc_set_stream.argtypes = [VP, VP]
+        L.jfc_kernel_launches.restype = ctypes.c_ulonglong
+        L.jfc_get_params.argtypes = [VP, ctypes.POINTER(Params)]
+        L.jfc_default_params.argtypes = [ctypes.POINTER(Params)]
+        L.jfc_default_params.restype = None
+        L.jfc_default_model.argtypes = [ctypes.POINTER(Model)]
+        L.jfc_default_model.restype = None
+        L.jfc_graph_create_grid.argtypes = [VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, ctypes.POINTER(VP)]
+        L.jfc_graph_destroy.argtypes = [VP]
+        L.jfc_graph_destroy.restype = None
+        L.jfc_graph_build_from_image.argtypes = [VP, VP, ctypes.c_int, U8P, ctypes.POINTER(Model)]
+        L.jfc_graph_build_from_device.argtypes = [VP, VP, ctypes.c_int, VP, ctypes.POINTER(Model)]
+        L.jfc_graph_set.argtypes = [VP, I32P, ctypes.POINTER(I32P), ctypes.c_int64]
+        L.jfc_graph_set_device.argtypes = [VP, VP, ctypes.POINTER(VP), ctypes.c_int64]
+        L.jfc_graph_get_state.argtypes = [VP, I32P, ctypes.POINTER(I32P), I32P]
+        L.jfc_solve.argtypes = [VP, ctypes.POINTER(Stats)]
+        L.jfc_get_flow.argtypes = [VP, ctypes.POINTER(ctypes.c_int64)]
+        L.jfc_read_labels.argtypes = [VP, U8P]
+        L.jfc_read_labels_device.argtypes = [VP, VP]
+        L.jfc_edit_tlinks.argtypes = [VP, U32P, I32P, I32P, ctypes.c_size_t]
+        L.jfc_graph_edit_seeds.argtypes = [VP, U32P, U8P, ctypes.c_size_t]
+        L.jfc_batch_create.argtypes = [VP, ctypes.POINTER(VP)]
+        L.jfc_batch_destroy.argtypes = [VP]
+        L.jfc_batch_destroy.restype = None
+        L.jfc_batch_add.argtypes = [VP, VP]
+        L.jfc_batch_clear.argtypes = [VP]
+        L.jfc_batch_size.argtypes = [VP]
+        L.jfc_batch_solve.argtypes = [VP, ctypes.POINTER(Stats)]
+        L.jfc_batch_autotune.argtypes = [VP, ctypes.POINTER(Params)]
+        L.jfc_server_create.argtypes = [VP, ctypes.c_size_t, ctypes.c_int, ctypes.POINTER(VP)]
+        L.jfc_server_destroy.argtypes = [VP]
+        L.jfc_server_destroy.restype = None
+        L.jfc_server_submit.argtypes = [VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, VP,
+                                        ctypes.c_int, U8P, ctypes.POINTER(Model), ctypes.POINTER(ctypes.c_int)]
+        L.jfc_server_edit.argtypes = [VP, ctypes.c_int, U32P, U8P, ctypes.c_size_t]
+        L.jfc_server_wait.argtypes = [VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(RequestInfo)]
+        L.jfc_server_read_labels.argtypes = [VP, ctypes.c_int, U8P]
+        L.jfc_server_close.argtypes = [VP, ctypes.c_int]
+        L.jfc_server_cancel.argtypes = [VP, ctypes.c_int]
+        L.jfc_synth_gray_ellipse.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int, U8P, U8P]
+        L.jfc_synth_rgb_ellipses.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int, U8P, U8P]
+        L.jfc_synth_rgb_video.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64, U8P, U8P]
+        L.jfc_synth_i16_phantom.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
+                                            ctypes.c_int, ctypes.POINTER(ctypes.c_int16), U8P]
+        L.jfc_synth_stroke.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
+                                       ctypes.c_size_t, ctypes.c_uint8, U32P, U8P,
+                                       ctypes.POINTER(ctypes.c_size_t)]
+        _LIB = L
+    return _LIB
+
+
+def lib():
+    return _lib()
+
+
+def _check(rc, where):
+    if rc != OK:
+        raise JfcError(rc, where)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def kernel_launches():
+    return int(_lib().jfc_kernel_launches())
+
+
+def default_params(**kw):
+    p = Params()
+    _lib().jfc_default_params(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, int(v))
+    return p
+
+
+def default_model(**kw):
+    m = Model()
+    _lib().jfc_default_model(ctypes.byref(m))
+    for k, v in kw.items():
+        setattr(m, k, int(v))
+    return m
+
+
+def model_dict(m):
+    return {k: getattr(m, k) for k, _ in Model._fields_}
+
+
+class Context:
+    """One device + stream (QGCWidget::initContext / initOpenCL, QGCWidget.cpp:686-813)."""
+
+    def __init__(self, device=0, **params):
+        self.handle = VP()
+        p = default_params(**params)
+        _check(_lib().jfc_create(device, ctypes.byref(p), ctypes.byref(self.handle)), "jfc_create")
+
+    def set_params(self, **params):
+        p = self.params()
+        for k, v in params.items():
+            setattr(p, k, int(v))
+        _check(_lib().jfc_set_params(self.handle, ctypes.byref(p)), "jfc_set_params")
+
+    def set_stream(self, stream_ptr):
+        """Run this context's work on a caller-owned cudaStream_t (int pointer; 0 = own)."""
+        _check(_lib().jfc_set_stream(self.handle, VP(stream_ptr or None)), "jfc_set_stream")
+
+    def params(self):
+        p = Params()
+        _check(_lib().jfc_get_params(self.handle, ctypes.byref(p)), "jfc_get_params")
+        return p
+
+    def close(self):
+        if self.handle:
+            _lib().jfc_destroy(self.handle)
+            self.handle = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Graph:
+    """A 4-connected 2D or 6-connected 3D grid graph resident on the device.
+
+    shape: (H, W) or (D, H, W).  Residual arcs follow the reference channel
+    order (+x, +y, -y, -x) / (+x, +y, +z, -z, -y, -x)."""
+
+    def __init__(self, ctx, shape):
+        self.ctx = ctx
+        self.shape = tuple(int(s) for s in shape)
+        if len(self.shape) == 2:
+            self.dims, (self.h, self.w), self.d, self.conn = 2, self.shape, 1, 4
+        else:
+            self.dims, (self.d, self.h, self.w), self.conn = 3, self.shape, 6
+        self.n = self.w * self.h * self.d
+        self.handle = VP()
+        _check(_lib().jfc_graph_create_grid(ctx.handle, self.dims, self.w, self.h, self.d, self.conn,
+                                            ctypes.byref(self.handle)), "jfc_graph_create_grid")
+
+    # -- build (slotModelClicked: computeCapacity + kmeans + computeExcessFlowLazy)
+    def build_from_image(self, img, seeds, pixfmt, model=None):
+        img = np.ascontiguousarray(img)
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint8)
+        if seeds.size != self.n:
+            raise ValueError("seeds size mismatch")
+        m = model if isinstance(model, Model) else default_model(**(model or {}))
+        _check(_lib().jfc_graph_build_from_image(self.handle, img.ctypes.data_as(VP), int(pixfmt),
+                                                 _p(seeds, U8P), ctypes.byref(m)), "jfc_graph_build_from_image")
+
+    slotModelClicked = build_from_image
+
+    def build_from_device(self, d_img_ptr, d_seeds_ptr, pixfmt, model=None):
+        m = model if isinstance(model, Model) else default_model(**(model or {}))
+        _check(_lib().jfc_graph_build_from_device(self.handle, VP(d_img_ptr), int(pixfmt), VP(d_seeds_ptr),
+                                                  ctypes.byref(m)), "jfc_graph_build_from_device")
+
+    # -- explicit graph (slotLoadGraphClicked: .ef / .c1 / .c2)
+    def set(self, excess, caps, flow_offset=0):
+        e = np.ascontiguousarray(excess, dtype=np.int32).ravel()
+        cs = [np.ascontiguousarray(c, dtype=np.int32).ravel() for c in caps]
+        if len(cs) != self.conn or e.size != self.n or any(c.size != self.n for c in cs):
+            raise ValueError("graph arrays do not match the grid")
+        P = (I32P * self.conn)(*[_p(c, I32P) for c in cs])
+        _check(_lib().jfc_graph_set(self.handle, _p(e, I32P), P, int(flow_offset)), "jfc_graph_set")
+
+    slotLoadGraphClicked = set
+
+    def set_device(self, d_excess, d_caps, flow_offset=0):
+        P = (VP * self.conn)(*[VP(p) for p in d_caps])
+        _check(_lib().jfc_graph_set_device(self.handle, VP(d_excess), P, int(flow_offset)),
+               "jfc_graph_set_device")
+
+    # -- solve (slotCutClicked)
+    def solve(self):
+        st = Stats()
+        rc = _lib().jfc_solve(self.handle, ctypes.byref(st))
+        _check(rc, "jfc_solve")
+        return st
+
+    slotCutClicked = solve
+
+    def flow(self):
+        f = ctypes.c_int64()
+        _check(_lib().jfc_get_flow(self.handle, ctypes.byref(f)), "jfc_get_flow")
+        return f.value
+
+    def labels(self):
+        out = np.empty(self.n, np.uint8)
+        _check(_lib().jfc_read_labels(self.handle, _p(out, U8P)), "jfc_read_labels")
+        return out.reshape(self.shape)
+
+    def read_labels_device(self, d_out_ptr):
+        _check(_lib().jfc_read_labels_device(self.handle, VP(d_out_ptr)), "jfc_read_labels_device")
+
+    def state(self):
+        e = np.empty(self.n, np.int32)
+        h = np.empty(self.n, np.int32)
+        r = [np.empty(self.n, np.int32) for _ in range(self.conn)]
+        P = (I32P * self.conn)(*[_p(c, I32P) for c in r])
+        _check(_lib().jfc_graph_get_state(self.handle, _p(e, I32P), P, _p(h, I32P)), "jfc_graph_get_state")
+        return e, r, h
+
+    # -- warm edits
+    def edit_tlinks(self, idx, dcs, dct):
+        idx = np.ascontiguousarray(idx, dtype=np.uint32)
+        dcs = np.ascontiguousarray(dcs, dtype=np.int32)
+        dct = np.ascontiguousarray(dct, dtype=np.int32)
+        _check(_lib().jfc_edit_tlinks(self.handle, _p(idx, U32P), _p(dcs, I32P), _p(dct, I32P), idx.size),
+               "jfc_edit_tlinks")
+
+    def edit_seeds(self, idx, new_seed):
+        idx = np.ascontiguousarray(idx, dtype=np.uint32)
+        ns = np.ascontiguousarray(new_seed, dtype=np.uint8)
+        _check(_lib().jfc_graph_edit_seeds(self.handle, _p(idx, U32P), _p(ns, U8P), idx.size),
+               "jfc_graph_edit_seeds")
+
+    def close(self):
+        if self.handle:
+            _lib().jfc_graph_destroy(self.handle)
+            self.handle = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent grids solved together (one persistent launch per phase)."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self.handle = VP()
+        self.graphs = []
+        _check(_lib().jfc_batch_create(ctx.handle, ctypes.byref(self.handle)), "jfc_batch_create")
+
+    def add(self, g):
+        _check(_lib().jfc_batch_add(self.handle, g.handle), "jfc_batch_add")
+        self.graphs.append(g)
+
+    def clear(self):
+        _check(_lib().jfc_batch_clear(self.handle), "jfc_batch_clear")
+        self.graphs = []
+
+    def solve(self):
+        st = (Stats * max(1, len(self.graphs)))()
+        rc = _lib().jfc_batch_solve(self.handle, st)
+        _check(rc, "jfc_batch_solve")
+        return list(st)[:len(self.graphs)]
+
+    def autotune(self):
+        p = Params()
+        _check(_lib().jfc_batch_autotune(self.handle, ctypes.byref(p)), "jfc_batch_autotune")
+        return p
+
+    def close(self):
+        if self.handle:
+            _lib().jfc_batch_destroy(self.handle)
+            self.handle = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching server with HBM-budget admission and warm edits."""
+
+    def __init__(self, ctx, hbm_budget_bytes, max_slots=64):
+        self.ctx = ctx
+        self.handle = VP()
+        _check(_lib().jfc_server_create(ctx.handle, int(hbm_budget_bytes), int(max_slots),
+                                        ctypes.byref(self.handle)), "jfc_server_create")
+
+    def submit(self, img, seeds, pixfmt, model=None):
+        img = np.ascontiguousarray(img)
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint8)
+        if seeds.ndim == 2:
+            dims, (h, w), d = 2, seeds.shape, 1
+        else:
+            dims, (d, h, w) = 3, seeds.shape
+        m = model if isinstance(model, Model) else default_model(**(model or {}))
+        sid = ctypes.c_int(-1)
+        _check(_lib().jfc_server_submit(self.handle, dims, w, h, d, img.ctypes.data_as(VP), int(pixfmt),
+                                        _p(seeds, U8P), ctypes.byref(m), ctypes.byref(sid)), "jfc_server_submit")
+        return sid.value
+
+    def edit(self, sid, idx, new_seed):
+        idx = np.ascontiguousarray(idx, dtype=np.uint32)
+        ns = np.ascontiguousarray(new_seed, dtype=np.uint8)
+        _check(_lib().jfc_server_edit(self.handle, int(sid), _p(idx, U32P), _p(ns, U8P), idx.size),
+               "jfc_server_edit")
+
+    def wait(self, sid, timeout_ms=-1):
+        info = RequestInfo()
+        rc = _lib().jfc_server_wait(self.handle, int(sid), int(timeout_ms), ctypes.byref(info))
+        _check(rc, "jfc_server_wait")
+        return info
+
+    def labels(self, sid, shape):
+        out = np.empty(int(np.prod(shape)), np.uint8)
+        _check(_lib().jfc_server_read_labels(self.handle, int(sid), _p(out, U8P)), "jfc_server_read_labels")
+        return out.reshape(shape)
+
+    def close_session(self, sid):
+        _check(_lib().jfc_server_close(self.handle, int(sid)), "jfc_server_close")
+
+    def cancel(self, sid):
+        _check(_lib().jfc_server_cancel(self.handle, int(sid)), "jfc_server_cancel")
+
+    def close(self):
+        if self.handle:
+            _lib().jfc_server_destroy(self.handle)
+            self.handle = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- synthetic inputs
+def synth_gray_ellipse(w, h, seed=0, noise_sigma=20):
+    img = np.empty((h, w), np.uint8)
+    seeds = np.empty((h, w), np.uint8)
+    _check(_lib().jfc_synth_gray_ellipse(w, h, seed, noise_sigma, _p(img, U8P), _p(seeds, U8P)),
+           "jfc_synth_gray_ellipse")
+    return img, seeds
+
+
+def synth_rgb_ellipses(w, h, seed=0, n_ellipses=20, noise_sigma=15, stroke_permille_x10=50):
+    img = np.empty((h, w, 3), np.uint8)
+    seeds = np.empty((h, w), np.uint8)
+    _check(_lib().jfc_synth_rgb_ellipses(w, h, seed, n_ellipses, noise_sigma, stroke_permille_x10,
+                                         _p(img, U8P), _p(seeds, U8P)), "jfc_synth_rgb_ellipses")
+    return img, seeds
+
+
+def synth_rgb_video(w, h, frames, seed=0):
+    img = np.empty((frames, h, w, 3), np.uint8)
+    seeds = np.empty((frames, h, w), np.uint8)
+    _check(_lib().jfc_synth_rgb_video(w, h, frames, seed, _p(img, U8P), _p(seeds, U8P)), "jfc_synth_rgb_video")
+    return img, seeds
+
+
+def synth_i16_phantom(w, h, d, seed=0, noise_sigma=10):
+    img = np.empty((d, h, w), np.int16)
+    seeds = np.empty((d, h, w), np.uint8)
+    _check(_lib().jfc_synth_i16_phantom(w, h, d, seed, noise_sigma, img.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)),
+                                        _p(seeds, U8P)), "jfc_synth_i16_phantom")
+    return img, seeds
+
+
+def synth_stroke(shape, seed, n, label):
+    if len(shape) == 2:
+        dims, (h, w), d = 2, shape, 1
+    else:
+        dims, (d, h, w) = 3, shape
+    idx = np.empty(n, np.uint32)
+    ns = np.empty(n, np.uint8)
+    k = ctypes.c_size_t(0)
+    _check(_lib().jfc_synth_stroke(dims, w, h, d, seed, n, label, _p(idx, U32P), _p(ns, U8P), ctypes.byref(k)),
+           "jfc_synth_stroke")
+    return idx[:k.value].copy(), ns[:k.value].copy()

@@ -1,0 +1,88 @@
+"""Shared test setup.  `-m gpu` tests need a B200 and call the CUDA library
+through its C ABI; everything else runs on the CPU."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "jf-cut_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+for p in (PKG, ORACLE, ROOT):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+FIXTURES = ("flower", "person", "sponge")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+    config.addinivalue_line("markers", "slow: long-running full-size case")
+
+
+def _ensure_built():
+    if not os.path.exists(os.path.join(PKG, "libjfcut.so")):
+        subprocess.run(["make", "-s", "-j8", "-C", PKG], check=True)
+    if not os.path.exists(os.path.join(ORACLE, "liboracle.so")):
+        subprocess.run(["make", "-s", "-f", os.path.join(ORACLE, "Makefile")], check=True, cwd=ORACLE)
+
+
+_ensure_built()
+
+
+def load_fixture(name):
+    """Golden graph from the reference data: (shape, excess, caps[4], maxflow, ref_object)."""
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    w, h = int(z["width"]), int(z["height"])
+    px = z["caps_px"].astype(np.int32).reshape(h, w)
+    py = z["caps_py"].astype(np.int32).reshape(h, w)
+    mx = np.zeros_like(px)
+    mx[:, 1:] = px[:, :-1]
+    my = np.zeros_like(py)
+    my[1:] = py[:-1]
+    caps = [px.ravel(), py.ravel(), my.ravel(), mx.ravel()]
+    return (h, w), z["excess"].astype(np.int32), caps, int(z["maxflow"]), z["ref_object"]
+
+
+def random_grid(shape, rng, cap_max=100, excess_max=300, density=0.5):
+    """Random folded grid graph (arcs leaving the grid are zero)."""
+    dims = len(shape)
+    n = int(np.prod(shape))
+    conn = 4 if dims == 2 else 6
+    caps = [rng.integers(0, cap_max + 1, n).astype(np.int32) for _ in range(conn)]
+    mask = rng.random(n) < density
+    e = np.where(mask, rng.integers(-excess_max, excess_max + 1, n), 0).astype(np.int32)
+    zero_boundary(shape, caps)
+    return e, caps
+
+
+def zero_boundary(shape, caps):
+    if len(shape) == 2:
+        h, w = shape
+        c = [x.reshape(h, w) for x in caps]
+        c[0][:, -1] = 0; c[1][-1, :] = 0; c[2][0, :] = 0; c[3][:, 0] = 0
+    else:
+        d, h, w = shape
+        c = [x.reshape(d, h, w) for x in caps]
+        c[0][:, :, -1] = 0; c[1][:, -1, :] = 0; c[2][-1] = 0
+        c[3][0] = 0; c[4][:, 0, :] = 0; c[5][:, :, 0] = 0
+
+
+def gpu_available():
+    try:
+        import jfcut
+        jfcut.Context(0).close()
+        return True
+    except Exception:
+        return False
+
+
+@pytest.fixture(scope="session")
+def ctx():
+    import jfcut
+    c = jfcut.Context(0)
+    yield c
+    c.close()

@@ -1,0 +1,254 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle (pinned
+to the reference), bit-exact on max-flow (int64) and the canonical cut."""
+import numpy as np
+import pytest
+
+import jfcut
+import oracle
+from conftest import FIXTURES, load_fixture, random_grid
+
+pytestmark = pytest.mark.gpu
+
+MODEL5 = dict(lambda_n=100, z_weight_pct=100, lambda_t=10, k_fg=5, k_bg=5, seed_cap=1000000, kmeans_iters=32)
+MODEL2 = dict(MODEL5, k_fg=2, k_bg=2)
+
+
+def solve_set(ctx, shape, e, caps, offset=0):
+    g = jfcut.Graph(ctx, shape)
+    g.set(e, caps, offset)
+    st = g.solve()
+    return g, st
+
+
+def check_against_oracle(shape, e, caps, flow, labels, offset=0):
+    f, _, _, lab = oracle.maxflow(shape, e, caps)
+    assert flow == f + offset
+    assert np.array_equal(labels.ravel(), lab)
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_golden_fixtures(ctx, name):
+    shape, e, caps, published, ref_obj = load_fixture(name)
+    g, st = solve_set(ctx, shape, e, caps)
+    assert st.status == 0
+    assert g.flow() == published
+    lab = g.labels().ravel()
+    _, _, _, olab = oracle.maxflow(shape, e, caps)
+    assert np.array_equal(lab, olab)
+    if ref_obj.sum():
+        assert np.array_equal(lab, ref_obj)    # the reference GPU's own cut
+    # the final residual state is a valid flow and its reachability is the cut
+    ef, r, _ = g.state()
+    assert oracle.check_residual(shape, e, caps, ef, r) == 0
+    lab2, bad = oracle.cut_from_residual(shape, ef, r)
+    assert bad == 0 and np.array_equal(lab2, lab)
+
+
+@pytest.mark.parametrize("tile_rows,local_iters,interval", [(8, 1, 1), (16, 4, 2), (8, 32, 16), (16, 16, 8)])
+def test_schedules_agree(ctx, tile_rows, local_iters, interval):
+    ctx.set_params(tile_rows=tile_rows, local_iters=local_iters, relabel_interval=interval)
+    try:
+        shape, e, caps, published, _ = load_fixture("sponge")
+        g, st = solve_set(ctx, shape, e, caps)
+        assert g.flow() == published
+        _, _, _, olab = oracle.maxflow(shape, e, caps)
+        assert np.array_equal(g.labels().ravel(), olab)
+    finally:
+        ctx.set_params(tile_rows=16, local_iters=16, relabel_interval=8)
+
+
+SHAPES = [(1, 1), (1, 37), (37, 1), (17, 33), (16, 32), (33, 65), (100, 1000), (257, 131),
+          (1, 1, 1), (5, 5, 5), (3, 17, 9), (8, 33, 31), (13, 40, 70), (1, 1, 40), (40, 1, 1)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("seed", [0, 1])
+def test_random_grids(ctx, shape, seed):
+    rng = np.random.default_rng(1000 + seed)
+    e, caps = random_grid(shape, rng, cap_max=50 if seed else 1000, density=0.3 if seed else 0.8)
+    g, st = solve_set(ctx, shape, e, caps, offset=seed * 7)
+    check_against_oracle(shape, e, caps, g.flow(), g.labels(), offset=seed * 7)
+
+
+def test_long_paths(ctx):
+    # a serpentine corridor: flow has to travel across many tiles
+    h, w = 96, 200
+    n = h * w
+    caps = [np.zeros(n, np.int32) for _ in range(4)]
+    c = [x.reshape(h, w) for x in caps]
+    for y in range(0, h, 2):
+        c[0][y, :-1] = 5; c[3][y, 1:] = 5
+        x = w - 1 if (y // 2) % 2 == 0 else 0
+        if y + 2 < h:
+            c[1][y, x] = 5; c[2][y + 1, x] = 5
+            c[1][y + 1, x] = 5; c[2][y + 2, x] = 5
+    e = np.zeros(n, np.int32)
+    e[0] = 1000
+    e[(h - 2) * w + (w - 1 if ((h - 2) // 2) % 2 == 0 else 0)] = -1000
+    g, st = solve_set(ctx, (h, w), e, caps)
+    check_against_oracle((h, w), e, caps, g.flow(), g.labels())
+    assert g.flow() == 5
+
+
+def test_gray_ellipse_build_and_solve(ctx):
+    img, seeds = jfcut.synth_gray_ellipse(512, 512, seed=3)
+    g = jfcut.Graph(ctx, img.shape)
+    g.build_from_image(img, seeds, jfcut.PIX_GRAY8, MODEL2)
+    e_dev, r_dev, _ = g.state()
+    e, caps, st = oracle.build_graph(img, seeds, 0, MODEL2)
+    assert np.array_equal(e_dev, e)
+    for k in range(4):
+        assert np.array_equal(r_dev[k], caps[k])
+    s = g.solve()
+    check_against_oracle(img.shape, e, caps, g.flow(), g.labels(), offset=st)
+
+
+@pytest.mark.parametrize("w,h,seed", [(257, 131, 1), (640, 480, 2), (33, 1000, 3)])
+def test_rgb_build_and_solve(ctx, w, h, seed):
+    img, seeds = jfcut.synth_rgb_ellipses(w, h, seed=seed)
+    g = jfcut.Graph(ctx, (h, w))
+    g.build_from_image(img, seeds, jfcut.PIX_RGB8, MODEL5)
+    e_dev, r_dev, _ = g.state()
+    e, caps, st = oracle.build_graph(img, seeds, 1, MODEL5)
+    assert np.array_equal(e_dev, e)
+    assert all(np.array_equal(r_dev[k], caps[k]) for k in range(4))
+    g.solve()
+    check_against_oracle((h, w), e, caps, g.flow(), g.labels(), offset=st)
+
+
+def test_video_build_and_solve(ctx):
+    img, seeds = jfcut.synth_rgb_video(96, 64, 8, seed=4)
+    model = dict(MODEL5, z_weight_pct=50)
+    g = jfcut.Graph(ctx, seeds.shape)
+    g.build_from_image(img, seeds, jfcut.PIX_RGB8, model)
+    e_dev, r_dev, _ = g.state()
+    e, caps, st = oracle.build_graph(img, seeds, 1, model)
+    assert np.array_equal(e_dev, e)
+    assert all(np.array_equal(r_dev[k], caps[k]) for k in range(6))
+    g.solve()
+    check_against_oracle(seeds.shape, e, caps, g.flow(), g.labels(), offset=st)
+
+
+def test_i16_phantom_build_and_solve(ctx):
+    img, seeds = jfcut.synth_i16_phantom(40, 36, 28, seed=5)
+    g = jfcut.Graph(ctx, seeds.shape)
+    g.build_from_image(img, seeds, jfcut.PIX_I16, MODEL2)
+    e_dev, r_dev, _ = g.state()
+    e, caps, st = oracle.build_graph(img, seeds, 2, MODEL2)
+    assert np.array_equal(e_dev, e)
+    assert all(np.array_equal(r_dev[k], caps[k]) for k in range(6))
+    g.solve()
+    check_against_oracle(seeds.shape, e, caps, g.flow(), g.labels(), offset=st)
+
+
+def test_warm_seed_edits(ctx):
+    img, seeds = jfcut.synth_rgb_ellipses(300, 200, seed=11)
+    g = jfcut.Graph(ctx, seeds.shape)
+    g.build_from_image(img, seeds, jfcut.PIX_RGB8, MODEL5)
+    g.solve()
+    cur = seeds.copy().ravel()
+    for k in range(3):
+        idx, ns = jfcut.synth_stroke(seeds.shape, seed=50 + k, n=600, label=1 + (k % 2))
+        g.edit_seeds(idx, ns)
+        g.solve()
+        cur[idx] = ns
+        # cold reference: rebuild from scratch with the edited seeds but the ORIGINAL colour model
+        # is what the warm path keeps; compare against a cold GPU solve of the same edited graph
+        e_dev, r_dev, _ = g.state()
+        cold = jfcut.Graph(ctx, seeds.shape)
+        cold.build_from_image(img, seeds, jfcut.PIX_RGB8, MODEL5)
+        cold.edit_seeds(np.nonzero(cur != seeds.ravel())[0], cur[cur != seeds.ravel()])
+        e0, c0, _ = cold.state()
+        cold.solve()
+        assert g.flow() == cold.flow()
+        assert np.array_equal(g.labels(), cold.labels())
+        # and both equal the oracle on the edited graph
+        f, _, _, lab = oracle.maxflow(seeds.shape, e0, c0)
+        assert np.array_equal(g.labels().ravel(), lab)
+        cold.close()
+
+
+def test_edit_tlinks_deltas(ctx):
+    rng = np.random.default_rng(3)
+    shape = (70, 90)
+    e, caps = random_grid(shape, rng)
+    g, _ = solve_set(ctx, shape, e, caps)
+    idx = rng.choice(e.size, 300, replace=False).astype(np.uint32)
+    dcs = rng.integers(0, 200, 300).astype(np.int32)
+    dct = rng.integers(0, 200, 300).astype(np.int32)
+    g.edit_tlinks(idx, dcs, dct)
+    g.solve()
+    e2 = e.copy()
+    e2[idx] += dcs - dct
+    offset = int(np.minimum(dcs, dct).sum())
+    # sum ct grows by dct; the folded oracle sees e2 with the extra min(dcs, dct) offset
+    f, _, _, lab = oracle.maxflow(shape, e2, caps)
+    # flow of the edited graph = sum_i min(cs', ct') + folded flow; with e given as net excess
+    cs0 = np.maximum(e, 0).astype(np.int64); ct0 = np.maximum(-e, 0).astype(np.int64)
+    cs1 = cs0.copy(); ct1 = ct0.copy()
+    np.add.at(cs1, idx, dcs); np.add.at(ct1, idx, dct)
+    assert g.flow() == f + int(np.minimum(cs1, ct1).sum())
+    assert np.array_equal(g.labels().ravel(), lab)
+
+
+def test_batch_matches_plain(ctx):
+    rng = np.random.default_rng(8)
+    b = jfcut.Batch(ctx)
+    graphs, refs = [], []
+    for i in range(12):
+        w, h = int(rng.integers(20, 300)), int(rng.integers(20, 300))
+        img, seeds = jfcut.synth_rgb_ellipses(w, h, seed=100 + i)
+        g = jfcut.Graph(ctx, (h, w))
+        g.build_from_image(img, seeds, jfcut.PIX_RGB8, MODEL5)
+        e, caps, st = oracle.build_graph(img, seeds, 1, MODEL5)
+        refs.append((e, caps, st))
+        graphs.append(g)
+        b.add(g)
+    # one 3D grid in the same batch
+    img, seeds = jfcut.synth_i16_phantom(20, 24, 16, seed=9)
+    g3 = jfcut.Graph(ctx, seeds.shape)
+    g3.build_from_image(img, seeds, jfcut.PIX_I16, MODEL2)
+    e3, c3, st3 = oracle.build_graph(img, seeds, 2, MODEL2)
+    b.add(g3)
+    stats = b.solve()
+    assert all(s.status == 0 for s in stats)
+    for g, (e, caps, st) in zip(graphs, refs):
+        check_against_oracle(g.shape, e, caps, g.flow(), g.labels(), offset=st)
+    check_against_oracle(g3.shape, e3, c3, g3.flow(), g3.labels(), offset=st3)
+
+
+def test_errors(ctx):
+    img, seeds = jfcut.synth_gray_ellipse(64, 64, seed=1)
+    g = jfcut.Graph(ctx, img.shape)
+    with pytest.raises(jfcut.JfcError) as ei:
+        g.solve()
+    assert ei.value.code == jfcut.ERR_STATE
+    s2 = seeds.copy()
+    s2[s2 == 2] = 0
+    with pytest.raises(jfcut.JfcError) as ei:
+        g.build_from_image(img, s2, jfcut.PIX_GRAY8)
+    assert ei.value.code == jfcut.ERR_NO_SEEDS
+    with pytest.raises(jfcut.JfcError) as ei:
+        g.labels()
+    assert ei.value.code == jfcut.ERR_STATE
+    with pytest.raises(jfcut.JfcError) as ei:
+        jfcut.Graph(ctx, (0, 5))
+    assert ei.value.code == jfcut.ERR_INVALID_ARG
+    bad = [np.full(4096, -1, np.int32)] * 4
+    with pytest.raises(jfcut.JfcError) as ei:
+        g.set(np.zeros(4096, np.int32), bad)
+    assert ei.value.code == jfcut.ERR_INVALID_ARG
+
+
+def test_budget_reports_not_converged(ctx):
+    # a one-sweep budget on a long-path instance must fail loudly, never return a cut silently
+    ctx.set_params(max_sweeps=1, relabel_interval=1, local_iters=1)
+    try:
+        shape, e, caps, published, _ = load_fixture("flower")
+        g = jfcut.Graph(ctx, shape)
+        g.set(e, caps)
+        with pytest.raises(jfcut.JfcError) as ei:
+            g.solve()
+        assert ei.value.code == jfcut.ERR_NOT_CONVERGED
+    finally:
+        ctx.set_params(max_sweeps=1 << 20, relabel_interval=8, local_iters=16)

@@ -242,11 +242,15 @@ def main():
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         visits, ms_pr, sweeps = 0, 0.0, 0
+        agg = {"ms_total": 0.0, "ms_push_relabel": 0.0, "ms_global_relabel": 0.0, "ms_cut": 0.0,
+               "global_relabels": 0, "bfs_passes": 0}
         for _ in range(args.steps):
             st = step_device()
             visits += st.tile_visits
             ms_pr += st.ms_push_relabel
             sweeps += st.sweeps
+            for k in agg:
+                agg[k] += getattr(st, k)
             assert g.flow() == flow_ref
         ev1.record(stream)
         barrier()
@@ -283,7 +287,9 @@ def main():
                        "nodes": n, "global_batch": world, "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (state %.1f GB)" % (jfcut.lib().jfc_graph_bytes(2, w, h, 1) / 1e9),
                        "params": {k: getattr(ctx.params(), k) for k in ("tile_rows", "local_iters", "relabel_interval")},
-                       "flow": flow_ref, "sweeps_per_step": sweeps / args.steps},
+                       "flow": flow_ref, "sweeps_per_step": sweeps / args.steps,
+                       "solve_breakdown_per_step": {k: v / args.steps for k, v in agg.items()},
+                       "pr_tile_visits_per_step": visits / args.steps},
             "e2e": {"value": e2e, "unit": "Mnodes/s", "h2d_bytes_per_step": int(img.nbytes + seeds.nbytes),
                     "d2h_bytes_per_step": int(n)},
             "gpu_launches": int(launches),

@@ -105,6 +105,8 @@ typedef struct jfc_stats {
   long long flow;         /* max-flow value (int64) */
   long long source_nodes; /* nodes on the source side */
   double ms_total, ms_build, ms_push_relabel, ms_global_relabel, ms_cut;
+  long long pr_rounds;    /* push/relabel rounds summed over tile visits */
+  long long bfs_visits;   /* tile visits of all BFS passes */
 } jfc_stats;
 
 typedef struct jfc_ctx jfc_ctx;

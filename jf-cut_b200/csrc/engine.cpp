@@ -79,8 +79,7 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDe
   }
   std::vector<GridDev> grids = grids_in;
   std::vector<int4> info;
-  std::vector<int> list[2];
-  int base = 0;
+  int base = 0, npar[2] = {0, 0};
   for (size_t gi = 0; gi < grids.size(); ++gi) {
     GridDev& g = grids[gi];
     if (g.dims != dims) return set_error(JFC_ERR_INVALID_ARG, "tile set mixes 2D and 3D grids");
@@ -92,46 +91,56 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDe
       for (int ty = 0; ty < g.tiles_y; ++ty)
         for (int tx = 0; tx < g.tiles_x; ++tx) {
           info.push_back(make_int4((int)gi, tx, ty, tz));
-          list[(tx + ty + tz) & 1].push_back(base + tx + g.tiles_x * (ty + g.tiles_y * tz));
+          ++npar[(tx + ty + tz) & 1];
         }
     base += g.tiles_x * g.tiles_y * g.tiles_z;
   }
   ts.ngrids = (int)grids.size();
   ts.ntiles = base;
-  ts.nlist[0] = (int)list[0].size();
-  ts.nlist[1] = (int)list[1].size();
+  ts.nlist[0] = npar[0];
+  ts.nlist[1] = npar[1];
+  const size_t nt = (size_t)ts.ntiles;
   size_t off = 0;
-  const size_t o_desc = off; off = align_up(off + sizeof(GridDev) * grids.size(), 256);
-  const size_t o_info = off; off = align_up(off + sizeof(int4) * info.size(), 256);
-  const size_t o_l0 = off; off = align_up(off + sizeof(int) * list[0].size(), 256);
-  const size_t o_l1 = off; off = align_up(off + sizeof(int) * list[1].size(), 256);
-  const size_t o_fpr = off; off = align_up(off + (size_t)ts.ntiles, 256);
-  const size_t o_fb0 = off; off = align_up(off + (size_t)ts.ntiles, 256);
-  const size_t o_fb1 = off; off = align_up(off + (size_t)ts.ntiles, 256);
-  const size_t o_act = off; off = align_up(off + sizeof(int) * grids.size(), 256);
-  const size_t o_sum = off; off = align_up(off + sizeof(long long) * 2 * grids.size(), 256);
-  const size_t o_ctr = off; off = align_up(off + sizeof(DevCounters), 256);
+  auto take = [&](size_t bytes) { const size_t o = off; off = align_up(off + bytes, 256); return o; };
+  const size_t o_desc = take(sizeof(GridDev) * grids.size());
+  const size_t o_info = take(sizeof(int4) * nt);
+  const size_t o_fpr = take(sizeof(int) * nt);
+  size_t o_qpr[2][2];
+  for (int p = 0; p < 2; ++p)
+    for (int b = 0; b < 2; ++b) o_qpr[p][b] = take(sizeof(int) * (size_t)npar[p]);
+  const size_t o_fb0 = take(sizeof(int) * nt);
+  const size_t o_fb1 = take(sizeof(int) * nt);
+  const size_t o_qb0 = take(sizeof(int) * nt);
+  const size_t o_qb1 = take(sizeof(int) * nt);
+  unsigned cap = 32;
+  while (cap < (unsigned)nt) cap <<= 1;
+  const size_t o_wq = take(sizeof(unsigned long long) * cap);
+  const size_t o_act = take(nt);
+  const size_t o_gact = take(sizeof(int) * grids.size());
+  const size_t o_sum = take(sizeof(long long) * 2 * grids.size());
+  const size_t o_ctr = take(sizeof(DevCounters));
   char* blk = nullptr;
   JFC_CUDA(cudaMalloc((void**)&blk, off));
   ts.d_block = blk;
   ts.block_bytes = off;
   ts.d_desc = (GridDev*)(blk + o_desc);
   ts.d_info = (int4*)(blk + o_info);
-  ts.d_list[0] = (int*)(blk + o_l0);
-  ts.d_list[1] = (int*)(blk + o_l1);
-  ts.d_flag_pr = (uint8_t*)(blk + o_fpr);
-  ts.d_flag_bfs[0] = (uint8_t*)(blk + o_fb0);
-  ts.d_flag_bfs[1] = (uint8_t*)(blk + o_fb1);
-  ts.d_grid_active = (int*)(blk + o_act);
+  ts.d_flag_pr = (int*)(blk + o_fpr);
+  for (int p = 0; p < 2; ++p)
+    for (int b = 0; b < 2; ++b) ts.d_q_pr[p][b] = (int*)(blk + o_qpr[p][b]);
+  ts.d_flag_bfs[0] = (int*)(blk + o_fb0);
+  ts.d_flag_bfs[1] = (int*)(blk + o_fb1);
+  ts.d_q_bfs[0] = (int*)(blk + o_qb0);
+  ts.d_q_bfs[1] = (int*)(blk + o_qb1);
+  ts.d_act = (uint8_t*)(blk + o_act);
+  ts.d_wq = (unsigned long long*)(blk + o_wq);
+  ts.wq_cap = cap;
+  ts.d_grid_active = (int*)(blk + o_gact);
   ts.d_grid_sum = (long long*)(blk + o_sum);
   ts.d_ctr = (DevCounters*)(blk + o_ctr);
   JFC_CUDA(cudaMemset(blk, 0, off));
   JFC_CUDA(cudaMemcpy(ts.d_desc, grids.data(), sizeof(GridDev) * grids.size(), cudaMemcpyHostToDevice));
   JFC_CUDA(cudaMemcpy(ts.d_info, info.data(), sizeof(int4) * info.size(), cudaMemcpyHostToDevice));
-  if (!list[0].empty())
-    JFC_CUDA(cudaMemcpy(ts.d_list[0], list[0].data(), sizeof(int) * list[0].size(), cudaMemcpyHostToDevice));
-  if (!list[1].empty())
-    JFC_CUDA(cudaMemcpy(ts.d_list[1], list[1].data(), sizeof(int) * list[1].size(), cudaMemcpyHostToDevice));
   return JFC_OK;
 }
 
@@ -146,46 +155,40 @@ static int pin_reserve(jfc_ctx* ctx, size_t bytes) {
   return JFC_OK;
 }
 
-// Run one BFS (global relabel when !cut, cut otherwise) to its fixpoint.
-// On return (relabel) active[g] holds the active tiles of every grid.
+// Run one BFS (global relabel when !cut, cut otherwise) to its fixpoint in
+// one persistent launch, then read back its outcome (the only host sync of a
+// relabel cycle).  On return (relabel) active[g] holds the active tiles of
+// every grid.
 static int run_bfs(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, bool cut, int& passes,
-                   std::vector<int>* active, int* cut_bad) {
+                   std::vector<int>* active, int* cut_bad, cudaEvent_t ev_done, int* sweeps_done) {
   cudaStream_t s = ctx->stream;
-  JFC_CUDA(cudaMemsetAsync(ts.d_flag_bfs[0], 0, (size_t)ts.ntiles, s));
-  JFC_CUDA(cudaMemsetAsync(ts.d_flag_bfs[1], 0, (size_t)ts.ntiles, s));
+  JFC_CUDA(cudaMemsetAsync(ts.d_flag_bfs[0], 0, sizeof(int) * (size_t)ts.ntiles, s));
+  JFC_CUDA(cudaMemsetAsync(ts.d_flag_bfs[1], 0, sizeof(int) * (size_t)ts.ntiles, s));
   if (!cut) JFC_CUDA(cudaMemsetAsync(ts.d_grid_active, 0, sizeof(int) * ts.ngrids, s));
-  else JFC_CUDA(cudaMemsetAsync(&ts.d_ctr->cut_bad, 0, sizeof(int), s));
-  JFC_CUDA(cut ? launch_cut_pass(ts, 0, true, s) : launch_relabel_pass(ts, 0, true, s));
-  int pass = 1, batch = 2;
-  const size_t need = sizeof(int) * (4 + (size_t)ts.ngrids);
+  // reset the BFS part of the control block: tickets, frontiers, status, cut flag
+  JFC_CUDA(cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s));
+  JFC_CUDA(cudaMemsetAsync(ts.d_ctr->qn_bfs, 0, sizeof(ts.d_ctr->qn_bfs), s));
+  JFC_CUDA(cudaMemsetAsync(&ts.d_ctr->bfs_status, 0, sizeof(int), s));
+  if (cut) JFC_CUDA(cudaMemsetAsync(&ts.d_ctr->cut_bad, 0, sizeof(int), s));
+  JFC_CUDA(launch_bfs(ts, cut, p.max_bfs_passes, s));
+  if (ev_done) JFC_CUDA(cudaEventRecord(ev_done, s));
+  const size_t need = sizeof(DevCounters) + sizeof(int) * (size_t)ts.ngrids + 64;
   int rc = pin_reserve(ctx, need);
   if (rc) return rc;
-  int* hp = (int*)ctx->h_pin;
-  for (;;) {
-    for (int k = 0; k < batch; ++k)
-      JFC_CUDA(cut ? launch_cut_pass(ts, pass + k, false, s) : launch_relabel_pass(ts, pass + k, false, s));
-    pass += batch;
-    JFC_CUDA(cudaMemcpyAsync(hp, &ts.d_ctr->pending[(pass - 1) & 1], sizeof(int), cudaMemcpyDeviceToHost, s));
-    JFC_CUDA(cudaStreamSynchronize(s));
-    if (hp[0] == 0) break;
-    if (pass > p.max_bfs_passes) {
-      passes += pass;
-      return set_error(JFC_ERR_NOT_CONVERGED, "BFS pass budget exhausted");
-    }
-    if (batch < 16) batch *= 2;
-  }
-  passes += pass;
+  DevCounters* hc = (DevCounters*)ctx->h_pin;
+  int* hact = (int*)((char*)ctx->h_pin + sizeof(DevCounters));
+  JFC_CUDA(cudaMemcpyAsync(hc, ts.d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+  if (!cut) JFC_CUDA(cudaMemcpyAsync(hact, ts.d_grid_active, sizeof(int) * ts.ngrids, cudaMemcpyDeviceToHost, s));
+  JFC_CUDA(cudaStreamSynchronize(s));
+  passes += hc->bfs_passes;
+  if (sweeps_done) *sweeps_done = hc->sweeps_done;
+  if (hc->error) return set_error(JFC_ERR_CUDA, "grid barrier timed out in a persistent kernel");
+  if (hc->bfs_status == 2) return set_error(JFC_ERR_NOT_CONVERGED, "BFS pass budget exhausted");
   if (!cut && active) {
     active->resize(ts.ngrids);
-    JFC_CUDA(cudaMemcpyAsync(hp + 4, ts.d_grid_active, sizeof(int) * ts.ngrids, cudaMemcpyDeviceToHost, s));
-    JFC_CUDA(cudaStreamSynchronize(s));
-    for (int g = 0; g < ts.ngrids; ++g) (*active)[g] = hp[4 + g];
+    for (int g = 0; g < ts.ngrids; ++g) (*active)[g] = hact[g];
   }
-  if (cut && cut_bad) {
-    JFC_CUDA(cudaMemcpyAsync(hp, &ts.d_ctr->cut_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
-    JFC_CUDA(cudaStreamSynchronize(s));
-    *cut_bad = hp[0];
-  }
+  if (cut && cut_bad) *cut_bad = hc->cut_bad;
   return JFC_OK;
 }
 
@@ -204,19 +207,18 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   cudaStream_t s = ctx->stream;
   std::memset(&st, 0, sizeof(st));
   res.assign(ts.ngrids, GridResult());
-  Timer t_all, t_ph;
+  Timer t_all, t_pr, t_gr, t_cut;
   JFC_CUDA(cudaEventRecord(t_all.a, s));
   JFC_CUDA(launch_clear_counters(ts, s));
   std::vector<int> active;
   int rc;
 
-  JFC_CUDA(cudaEventRecord(t_ph.a, s));
-  rc = run_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr);
-  JFC_CUDA(cudaEventRecord(t_ph.b, s));
-  JFC_CUDA(cudaEventSynchronize(t_ph.b));
-  st.ms_global_relabel += elapsed_ms(t_ph.a, t_ph.b);
-  st.global_relabels = 1;
+  // initial global relabel (exact sink distances; fills the work queues)
+  JFC_CUDA(cudaEventRecord(t_gr.a, s));
+  rc = run_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, t_gr.b, nullptr);
   if (rc) return rc;
+  st.ms_global_relabel += elapsed_ms(t_gr.a, t_gr.b);
+  st.global_relabels = 1;
 
   auto total = [&]() { long long t = 0; for (int v : active) t += v; return t; };
   int status = JFC_OK;
@@ -225,23 +227,20 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
       status = set_error(JFC_ERR_NOT_CONVERGED, "sweep budget exhausted");
       break;
     }
-    JFC_CUDA(cudaEventRecord(t_ph.a, s));
-    for (int k = 0; k < p.relabel_interval; ++k) {
-      JFC_CUDA(launch_pr_sweep(ts, 0, p.local_iters, s));
-      JFC_CUDA(launch_pr_sweep(ts, 1, p.local_iters, s));
-      ++st.sweeps;
-    }
-    JFC_CUDA(cudaEventRecord(t_ph.b, s));
-    JFC_CUDA(cudaEventSynchronize(t_ph.b));
-    st.ms_push_relabel += elapsed_ms(t_ph.a, t_ph.b);
-
-    JFC_CUDA(cudaEventRecord(t_ph.a, s));
-    rc = run_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr);
-    JFC_CUDA(cudaEventRecord(t_ph.b, s));
-    JFC_CUDA(cudaEventSynchronize(t_ph.b));
-    st.ms_global_relabel += elapsed_ms(t_ph.a, t_ph.b);
-    ++st.global_relabels;
+    // relabel_interval x (even sweep, odd sweep) in one persistent launch
+    JFC_CUDA(cudaEventRecord(t_pr.a, s));
+    JFC_CUDA(cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s));
+    JFC_CUDA(launch_pr_phase(ts, p.relabel_interval, p.local_iters, s));
+    JFC_CUDA(cudaEventRecord(t_pr.b, s));
+    // global relabel + active-tile count (one host read-back per cycle)
+    JFC_CUDA(cudaEventRecord(t_gr.a, s));
+    int sw = 0;
+    rc = run_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, t_gr.b, &sw);
     if (rc) return rc;
+    st.sweeps += sw;
+    st.ms_push_relabel += elapsed_ms(t_pr.a, t_pr.b);
+    st.ms_global_relabel += elapsed_ms(t_gr.a, t_gr.b);
+    ++st.global_relabels;
   }
   if (status != JFC_OK) {
     for (int g = 0; g < ts.ngrids; ++g)
@@ -250,22 +249,24 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
 
   // canonical cut: nodes reachable from excess in the final residual graph
   int bad = 0;
-  JFC_CUDA(cudaEventRecord(t_ph.a, s));
-  rc = run_bfs(ctx, ts, p, true, st.bfs_passes, nullptr, &bad);
+  JFC_CUDA(cudaEventRecord(t_cut.a, s));
+  rc = run_bfs(ctx, ts, p, true, st.bfs_passes, nullptr, &bad, nullptr, nullptr);
   if (rc) return rc;
   JFC_CUDA(launch_grid_sums(ts, s));
-  JFC_CUDA(cudaEventRecord(t_ph.b, s));
-  rc = pin_reserve(ctx, sizeof(long long) * 2 * (size_t)ts.ngrids + 64);
+  JFC_CUDA(cudaEventRecord(t_cut.b, s));
+  rc = pin_reserve(ctx, sizeof(long long) * 2 * (size_t)ts.ngrids + 128);
   if (rc) return rc;
   long long* hs = (long long*)ctx->h_pin;
+  unsigned long long* hv = (unsigned long long*)(hs + 2 * ts.ngrids);
   JFC_CUDA(cudaMemcpyAsync(hs, ts.d_grid_sum, sizeof(long long) * 2 * ts.ngrids, cudaMemcpyDeviceToHost, s));
-  unsigned long long visits = 0;
-  JFC_CUDA(cudaMemcpyAsync(&visits, &ts.d_ctr->visits, sizeof(visits), cudaMemcpyDeviceToHost, s));
+  JFC_CUDA(cudaMemcpyAsync(hv, &ts.d_ctr->visits, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   JFC_CUDA(cudaEventRecord(t_all.b, s));
   JFC_CUDA(cudaStreamSynchronize(s));
-  st.ms_cut = elapsed_ms(t_ph.a, t_ph.b);
+  st.ms_cut = elapsed_ms(t_cut.a, t_cut.b);
   st.ms_total = elapsed_ms(t_all.a, t_all.b);
-  st.tile_visits = (long long)visits;
+  st.tile_visits = (long long)hv[0];
+  st.bfs_visits = (long long)hv[1];
+  st.pr_rounds = (long long)hv[2];
   for (int g = 0; g < ts.ngrids; ++g) {
     res[g].neg_sum = hs[2 * g];
     res[g].labels = hs[2 * g + 1];

@@ -29,6 +29,7 @@ struct DevModel {
 
 struct jfc_graph {
   jfc_ctx* ctx = nullptr;
+  int device = 0;
   int dims = 2, W = 0, H = 0, D = 1, conn = 4;
   GridDev g{};                   // tile fields unset; pointers into d_state
   void* d_state = nullptr;

@@ -37,20 +37,27 @@ struct GridDev {
   uint8_t* label;
 };
 
-// Per-launch work-queue ticket (reset by the last block of each launch).
-struct Ticket {
-  unsigned int chunk;
-  unsigned int done;
-};
-
-// Device-side counters of one solve (one per tile set).
+// Device-side control state of one tile set (persistent phase kernels).
 struct DevCounters {
-  Ticket tk;                 // work queue ticket
-  int pending[2];            // BFS: a tile was flagged for the next pass
+  unsigned ticket[2];        // work tickets (alternate between phases)
+  unsigned bar_count;        // grid barrier arrivals
+  unsigned bar_gen;          // grid barrier generation
+  int error;                 // a barrier wait timed out: kernels leave, host reports
   int cut_bad;               // cut BFS reached a deficit node (augmenting path left)
+  int qn_pr[2][2];           // push-relabel queue lengths [parity][buffer]
+  int cur_pr[2];             // pending buffer per parity
+  int qn_bfs[2];             // BFS frontier lengths [buffer]
+  int bfs_passes;            // passes of the last BFS
+  int bfs_status;            // 1 converged, 2 pass budget exhausted
+  int sweeps_done;           // sweeps run by the last push-relabel phase
   int pad_;
   unsigned long long visits; // push-relabel tile visits
   unsigned long long bfs_visits;
+  unsigned long long rounds; // push/relabel rounds summed over visits
+  unsigned wq_head;          // BFS work list: next cell to take
+  unsigned wq_tail;          // BFS work list: next cell to fill
+  int wq_pending;            // work items pushed and not yet finished
+  int pad2_;
 };
 
 // A set of grids tiled with one tile shape: the unit every launch works on
@@ -62,10 +69,14 @@ struct TileSet {
   int ntiles = 0;
   GridDev* d_desc = nullptr;         // [ngrids]
   int4* d_info = nullptr;            // [ntiles] {grid, tx, ty, tz}
-  int* d_list[2] = {nullptr, nullptr};  // tile ids of parity 0 / 1
-  int nlist[2] = {0, 0};
-  uint8_t* d_flag_pr = nullptr;      // [ntiles] tile has active nodes
-  uint8_t* d_flag_bfs[2] = {nullptr, nullptr};  // [ntiles] BFS double buffer
+  int nlist[2] = {0, 0};             // tiles of parity 0 / 1
+  int* d_flag_pr = nullptr;          // [ntiles] tile waits in a push-relabel queue
+  int* d_q_pr[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [parity][buffer]
+  int* d_flag_bfs[2] = {nullptr, nullptr};  // [buffer][ntiles] tile waits in a BFS frontier
+  int* d_q_bfs[2] = {nullptr, nullptr};     // [buffer] BFS frontiers
+  unsigned long long* d_wq = nullptr;       // BFS work-list ring: (sequence << 32) | tile
+  unsigned wq_cap = 0;                      // ring size (power of two >= ntiles)
+  uint8_t* d_act = nullptr;          // [ntiles] tile held an active node at its last relabel visit
   int* d_grid_active = nullptr;      // [ngrids] active tiles after global relabel
   long long* d_grid_sum = nullptr;   // [ngrids*2] sum min(e,0), source-side count
   DevCounters* d_ctr = nullptr;
@@ -77,13 +88,15 @@ struct TileSet {
 void jfc_note_launch(int n = 1);
 
 // ----------------------------------------------------------- kernel launchers
-// (kernels_pr.cu)
-cudaError_t launch_pr_sweep(const TileSet& ts, int parity, int local_iters, cudaStream_t s);
-// (kernels_bfs.cu)
-cudaError_t launch_relabel_pass(const TileSet& ts, int pass, bool first, cudaStream_t s);
-cudaError_t launch_cut_pass(const TileSet& ts, int pass, bool first, cudaStream_t s);
+// (kernels_pr.cu) `sweeps` parity sweeps (even tiles, then odd tiles, ...)
+// in one persistent launch, draining the device work queues
+cudaError_t launch_pr_phase(const TileSet& ts, int sweeps, int local_iters, cudaStream_t s);
+// (kernels_bfs.cu) one BFS to its fixpoint in one persistent launch:
+// global relabel (cut = false; also refills the push-relabel queues) or the
+// source-side cut (cut = true)
+cudaError_t launch_bfs(const TileSet& ts, bool cut, int max_passes, cudaStream_t s);
 cudaError_t launch_grid_sums(const TileSet& ts, cudaStream_t s);
-cudaError_t launch_clear_counters(const TileSet& ts, cudaStream_t s);
+cudaError_t launch_clear_counters(const TileSet& ts, cudaStream_t s);  // also resets the work-list ring
 int persistent_blocks(const void* kernel, int threads, size_t smem);
 // layout helpers (kernels_bfs.cu)
 cudaError_t launch_fix_boundary(const GridDev& g, int conn, int* d_bad, cudaStream_t s);

@@ -26,11 +26,14 @@
 // shift-doubling closure and across rows is word AND/OR, so a tile converges
 // in a few word operations per row.  Reaching a deficit raises cut_bad (the
 // reference's done[1] divergence flag).
-#include "jfc_internal.h"
+#include "jfc_sync.cuh"
 
 namespace {
 
-constexpr unsigned FULL = 0xffffffffu;
+using jfc::FULL;
+
+// Work list the tile visits feed (deduplicated by its flags).
+using BfsQ = jfc::WorkList;
 
 template <int DIMS>
 struct Dirs {
@@ -68,202 +71,32 @@ __device__ __forceinline__ long long roff(const Addr& a, int i) {
   return a.base + (long long)(i % TY) * a.pitch + (long long)(i / TY) * a.slab;
 }
 
-// ------------------------------------------------------------ global relabel
-template <int DIMS, int TY, int TZ, bool FIRST>
-__device__ __forceinline__ void relabel_tile(const GridDev& g, int4 ti, int tid,
-                                             uint8_t* __restrict__ fnext, uint8_t* __restrict__ fpr,
-                                             int* __restrict__ pending, int& act_delta) {
-  using D = Dirs<DIMS>;
-  constexpr int R = TY * TZ;
+// Queue the neighbour tiles whose halo changed (rows_changed: rows of this
+// tile that changed; c0 / c31: a change in the first / last column) and the
+// tile itself when its in-tile fixpoint is not reached yet.
+template <int DIMS, int TY, int TZ>
+__device__ __forceinline__ void flag_neighbours(const GridDev& g, const Addr& a, int tid, unsigned rows_changed,
+                                                bool c0, bool c31, bool again, const BfsQ& Q) {
   const int lane = threadIdx.x & 31;
-  const Addr a = make_addr<DIMS, TY, TZ>(g, ti, lane);
-  const int* __restrict__ E = g.e;
-  int* __restrict__ H = g.h;
-  // residual-arc bits per row: bit k set when arc k is residual
-  unsigned arcs[R];
-  int h[R];
-  bool act_pos[R];
+  unsigned ymask0 = 0, ymask1 = 0, zmask0 = 0, zmask1 = 0;
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const long long n = roff<TY>(a, i);
-    const int e = E[n];
-    unsigned m = 0;
-    m |= (g.r[D::XP][n] > 0) ? 1u : 0u;
-    m |= (g.r[D::YP][n] > 0) ? 2u : 0u;
-    m |= (g.r[D::YM][n] > 0) ? 4u : 0u;
-    m |= (g.r[D::XM][n] > 0) ? 8u : 0u;
-    if constexpr (DIMS == 3) {
-      m |= (g.r[D::ZP][n] > 0) ? 16u : 0u;
-      m |= (g.r[D::ZM][n] > 0) ? 32u : 0u;
-    }
-    arcs[i] = m;
-    act_pos[i] = e > 0;
-    if constexpr (FIRST) h[i] = (e < 0) ? 0 : JFC_INF;
-    else h[i] = H[n];
+  for (int z = 0; z < TZ; ++z) { ymask0 |= 1u << (z * TY); ymask1 |= 1u << (z * TY + TY - 1); }
+#pragma unroll
+  for (int y = 0; y < TY; ++y) { zmask0 |= 1u << y; zmask1 |= 1u << ((TZ - 1) * TY + y); }
+  const int txs = g.tiles_x, tys = g.tiles_y;
+  bool want = false;
+  int nb = tid;
+  switch (lane) {
+    case 0: want = (rows_changed & ymask0) && a.has_yT; nb = tid - txs; break;
+    case 1: want = (rows_changed & ymask1) && a.has_yB; nb = tid + txs; break;
+    case 2: want = c0 && a.has_xL; nb = tid - 1; break;
+    case 3: want = c31 && a.has_xR; nb = tid + 1; break;
+    case 4: want = DIMS == 3 && (rows_changed & zmask0) && a.has_zT; nb = tid - txs * tys; break;
+    case 5: want = DIMS == 3 && (rows_changed & zmask1) && a.has_zB; nb = tid + txs * tys; break;
+    case 6: want = again; nb = tid; break;
+    default: break;
   }
-  // halo heights (FIRST: derived from neighbour excess)
-  auto halo = [&](long long n) -> int {
-    if constexpr (FIRST) return (E[n] < 0) ? 0 : JFC_INF;
-    else return H[n];
-  };
-  int hyT[TZ], hyB[TZ];
-  int hzT[DIMS == 3 ? TY : 1], hzB[DIMS == 3 ? TY : 1];
-#pragma unroll
-  for (int z = 0; z < TZ; ++z) {
-    const long long n = roff<TY>(a, z * TY);
-    hyT[z] = a.has_yT ? halo(n - a.pitch) : JFC_INF;
-    hyB[z] = a.has_yB ? halo(n + (long long)TY * a.pitch) : JFC_INF;
-  }
-  if constexpr (DIMS == 3) {
-#pragma unroll
-    for (int y = 0; y < TY; ++y) {
-      const long long n = roff<TY>(a, y);
-      hzT[y] = a.has_zT ? halo(n - a.slab) : JFC_INF;
-      hzB[y] = a.has_zB ? halo(n + (long long)TZ * a.slab) : JFC_INF;
-    }
-  }
-  int hs[R];
-  {
-    const int row = lane & 15;
-    const bool left = lane < 16;
-    int v = JFC_INF;
-    if (row < R && (left ? a.has_xL : a.has_xR)) {
-      const long long n = (long long)(left ? a.x0 - 1 : a.x0 + 32) +
-                          (long long)(a.y0 + row % TY) * a.pitch + (long long)(a.z0 + row / TY) * a.slab;
-      v = halo(n);
-    }
-#pragma unroll
-    for (int i = 0; i < R; ++i) {
-      const int lv = __shfl_sync(FULL, v, i);
-      const int rv = __shfl_sync(FULL, v, 16 + i);
-      hs[i] = (lane == 0) ? lv : rv;
-    }
-  }
-
-  unsigned dirty = 0;
-  bool converged = false;
-  auto relax_row = [&](int i) -> bool {
-    const int y = i % TY, z = i / TY;
-    int hxm = __shfl_up_sync(FULL, h[i], 1);
-    int hxp = __shfl_down_sync(FULL, h[i], 1);
-    if (lane == 0) hxm = hs[i];
-    if (lane == 31) hxp = hs[i];
-    const int hyp = (y < TY - 1) ? h[(i + 1 < R) ? i + 1 : i] : hyB[z];
-    const int hym = (y > 0) ? h[(i > 0) ? i - 1 : 0] : hyT[z];
-    const unsigned m = arcs[i];
-    int v = h[i];
-    if (m & 1u) v = min(v, hxp + 1);
-    if (m & 2u) v = min(v, hyp + 1);
-    if (m & 4u) v = min(v, hym + 1);
-    if (m & 8u) v = min(v, hxm + 1);
-    if constexpr (DIMS == 3) {
-      const int hzp = (z < TZ - 1) ? h[(i + TY < R) ? i + TY : i] : hzB[y];
-      const int hzm = (z > 0) ? h[(i >= TY) ? i - TY : 0] : hzT[y];
-      if (m & 16u) v = min(v, hzp + 1);
-      if (m & 32u) v = min(v, hzm + 1);
-    }
-    if (v < h[i]) { h[i] = v; dirty |= 1u << i; return true; }
-    return false;
-  };
-  for (int it = 0; it < 64; ++it) {
-    bool ch = false;
-#pragma unroll
-    for (int i = 0; i < R; ++i) ch |= relax_row(i);
-#pragma unroll
-    for (int i = R - 1; i >= 0; --i) ch |= relax_row(i);
-    if (!__any_sync(FULL, ch)) { converged = true; break; }
-  }
-
-#pragma unroll
-  for (int i = 0; i < R; ++i) {
-    if (FIRST || __any_sync(FULL, (dirty >> i) & 1u)) H[roff<TY>(a, i)] = h[i];
-  }
-  // flag neighbours whose halo fell, and myself if not yet at the fixpoint
-  unsigned rows_dirty = __reduce_or_sync(FULL, dirty);
-  const unsigned lane0 = __shfl_sync(FULL, dirty, 0);
-  const unsigned lane31 = __shfl_sync(FULL, dirty, 31);
-  bool act = false;
-#pragma unroll
-  for (int i = 0; i < R; ++i) act |= act_pos[i] & (h[i] < JFC_INF);
-  act = __any_sync(FULL, act);
-  if (lane == 0) {
-    unsigned ymask0 = 0, ymask1 = 0, zmask0 = 0, zmask1 = 0;
-#pragma unroll
-    for (int z = 0; z < TZ; ++z) { ymask0 |= 1u << (z * TY); ymask1 |= 1u << (z * TY + TY - 1); }
-#pragma unroll
-    for (int y = 0; y < TY; ++y) { zmask0 |= 1u << y; zmask1 |= 1u << ((TZ - 1) * TY + y); }
-    bool any = false;
-    const int txs = g.tiles_x, tys = g.tiles_y;
-    if ((rows_dirty & ymask0) && a.has_yT) { fnext[tid - txs] = 1; any = true; }
-    if ((rows_dirty & ymask1) && a.has_yB) { fnext[tid + txs] = 1; any = true; }
-    if (DIMS == 3) {
-      if ((rows_dirty & zmask0) && a.has_zT) { fnext[tid - txs * tys] = 1; any = true; }
-      if ((rows_dirty & zmask1) && a.has_zB) { fnext[tid + txs * tys] = 1; any = true; }
-    }
-    if (lane0 && a.has_xL) { fnext[tid - 1] = 1; any = true; }
-    if (lane31 && a.has_xR) { fnext[tid + 1] = 1; any = true; }
-    if (!converged) { fnext[tid] = 1; any = true; }
-    if (any) *pending = 1;
-    const int old = FIRST ? 0 : (int)fpr[tid];
-    fpr[tid] = act ? 1 : 0;
-    act_delta += (act ? 1 : 0) - old;
-  }
-}
-
-template <int DIMS, int TY, int TZ, bool FIRST>
-__global__ void __launch_bounds__(256) k_relabel(const GridDev* __restrict__ gd,
-                                                 const int4* __restrict__ info, int ntiles,
-                                                 uint8_t* __restrict__ fcur, uint8_t* __restrict__ fnext,
-                                                 uint8_t* __restrict__ fpr, int* __restrict__ grid_active,
-                                                 DevCounters* __restrict__ ctr, int pass) {
-  const int lane = threadIdx.x & 31;
-  if (blockIdx.x == 0 && threadIdx.x == 0) ctr->pending[(pass + 1) & 1] = 0;
-  int* pending = &ctr->pending[pass & 1];
-  int cur_grid = -1, delta = 0;
-  unsigned long long visits = 0;
-  for (;;) {
-    unsigned chunk = 0;
-    if (lane == 0) chunk = atomicAdd(&ctr->tk.chunk, 1u);
-    chunk = __shfl_sync(FULL, chunk, 0);
-    const long long b = (long long)chunk * 32;
-    if (b >= ntiles) break;
-    const long long li = b + lane;
-    bool f = li < ntiles;
-    if (!FIRST && f) {
-      f = fcur[li] != 0;
-      if (f) fcur[li] = 0;
-    }
-    unsigned m = __ballot_sync(FULL, f);
-    while (m) {
-      const int src = __ffs(m) - 1;
-      m &= m - 1;
-      const int tt = (int)b + src;
-      const int4 ti = info[tt];
-      if (ti.x != cur_grid) {
-        if (lane == 0 && delta != 0 && cur_grid >= 0) atomicAdd(&grid_active[cur_grid], delta);
-        delta = 0;
-        cur_grid = ti.x;
-      }
-      relabel_tile<DIMS, TY, TZ, FIRST>(gd[ti.x], ti, tt, fnext, fpr, pending, delta);
-      ++visits;
-    }
-  }
-  if (lane == 0 && delta != 0 && cur_grid >= 0) atomicAdd(&grid_active[cur_grid], delta);
-  __shared__ unsigned long long s_vis;
-  if (threadIdx.x == 0) s_vis = 0;
-  __syncthreads();
-  if (lane == 0 && visits) atomicAdd(&s_vis, visits);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if (s_vis) atomicAdd(&ctr->bfs_visits, s_vis);
-    __threadfence();
-    const unsigned prev = atomicAdd(&ctr->tk.done, 1u);
-    if (prev == gridDim.x - 1) {
-      ctr->tk.chunk = 0;
-      ctr->tk.done = 0;
-      __threadfence();
-    }
-  }
+  if (want) jfc::wl_push(Q, nb);
 }
 
 // ------------------------------------------------------------------ cut BFS
@@ -286,8 +119,7 @@ __device__ __forceinline__ unsigned close_left(unsigned p, unsigned m) {
 }
 
 template <int DIMS, int TY, int TZ, bool FIRST>
-__device__ __forceinline__ void cut_tile(const GridDev& g, int4 ti, int tid,
-                                         uint8_t* __restrict__ fnext, int* __restrict__ pending,
+__device__ __forceinline__ void cut_tile(const GridDev& g, int4 ti, int tid, const BfsQ& Q,
                                          int* __restrict__ bad) {
   using D = Dirs<DIMS>;
   constexpr int R = TY * TZ;
@@ -406,62 +238,44 @@ __device__ __forceinline__ void cut_tile(const GridDev& g, int4 ti, int tid,
     hit |= (L[i] & NEG[i]) != 0u;
     if (FIRST || c) Lb[roff<TY>(a, i)] = (uint8_t)((L[i] >> lane) & 1u);
   }
-  if (lane == 0) {
-    unsigned ymask0 = 0, ymask1 = 0, zmask0 = 0, zmask1 = 0;
-#pragma unroll
-    for (int z = 0; z < TZ; ++z) { ymask0 |= 1u << (z * TY); ymask1 |= 1u << (z * TY + TY - 1); }
-#pragma unroll
-    for (int y = 0; y < TY; ++y) { zmask0 |= 1u << y; zmask1 |= 1u << ((TZ - 1) * TY + y); }
-    // boundary labels that differ from what the neighbours last read (their
-    // halo read our labels, or our excess in the first pass)
-    const unsigned bnd = rows_changed;
-    const bool c0 = col0, c31 = col31;
-    bool any = false;
-    const int txs = g.tiles_x, tys = g.tiles_y;
-    if ((bnd & ymask0) && a.has_yT) { fnext[tid - txs] = 1; any = true; }
-    if ((bnd & ymask1) && a.has_yB) { fnext[tid + txs] = 1; any = true; }
-    if (DIMS == 3) {
-      if ((bnd & zmask0) && a.has_zT) { fnext[tid - txs * tys] = 1; any = true; }
-      if ((bnd & zmask1) && a.has_zB) { fnext[tid + txs * tys] = 1; any = true; }
-    }
-    if (c0 && a.has_xL) { fnext[tid - 1] = 1; any = true; }
-    if (c31 && a.has_xR) { fnext[tid + 1] = 1; any = true; }
-    if (!converged) { fnext[tid] = 1; any = true; }
-    if (any) *pending = 1;
-    if (hit) *bad = 1;
-  }
+  if (lane == 0 && hit) *bad = 1;
+  // boundary labels that differ from what the neighbours last read (their
+  // halo read our labels, or our excess in the first pass)
+  flag_neighbours<DIMS, TY, TZ>(g, a, tid, rows_changed, col0 != 0, col31 != 0, !converged, Q);
 }
 
-template <int DIMS, int TY, int TZ, bool FIRST>
-__global__ void __launch_bounds__(256) k_cut(const GridDev* __restrict__ gd,
-                                             const int4* __restrict__ info, int ntiles,
-                                             uint8_t* __restrict__ fcur, uint8_t* __restrict__ fnext,
-                                             DevCounters* __restrict__ ctr, int pass) {
+// Persistent cut BFS: the first pass visits every tile (labels start as
+// e > 0); then warps drain the work list (tiles whose halo labels changed),
+// one tile per warp, until nobody holds work and nothing is queued.
+template <int DIMS, int TY, int TZ>
+__global__ void __launch_bounds__(256) k_cut(TileSet ts, int max_passes) {
+  DevCounters* ctr = ts.d_ctr;
   const int lane = threadIdx.x & 31;
-  if (blockIdx.x == 0 && threadIdx.x == 0) ctr->pending[(pass + 1) & 1] = 0;
-  int* pending = &ctr->pending[pass & 1];
   unsigned long long visits = 0;
+  const BfsQ W{ts.d_wq, ts.wq_cap, ts.d_flag_bfs[0], ctr};
   for (;;) {
-    unsigned chunk = 0;
-    if (lane == 0) chunk = atomicAdd(&ctr->tk.chunk, 1u);
-    chunk = __shfl_sync(FULL, chunk, 0);
-    const long long b = (long long)chunk * 32;
-    if (b >= ntiles) break;
-    const long long li = b + lane;
-    bool f = li < ntiles;
-    if (!FIRST && f) {
-      f = fcur[li] != 0;
-      if (f) fcur[li] = 0;
-    }
-    unsigned m = __ballot_sync(FULL, f);
-    while (m) {
-      const int src = __ffs(m) - 1;
-      m &= m - 1;
-      const int tt = (int)b + src;
-      const int4 ti = info[tt];
-      cut_tile<DIMS, TY, TZ, FIRST>(gd[ti.x], ti, tt, fnext, pending, &ctr->cut_bad);
+    const unsigned c = jfc::warp_ticket(&ctr->ticket[0]);
+    const long long b = (long long)c * 32;
+    if (b >= ts.ntiles) break;
+    const int cnt = (int)min(32ll, (long long)ts.ntiles - b);
+    for (int k = 0; k < cnt; ++k) {
+      const int tt = (int)b + k;
+      const int4 ti = ts.d_info[tt];
+      cut_tile<DIMS, TY, TZ, true>(ts.d_desc[ti.x], ti, tt, W, &ctr->cut_bad);
       ++visits;
     }
+  }
+  bool ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
+  while (ok) {
+    int tt = 0;
+    if (lane == 0) tt = jfc::wl_pop(W);
+    tt = __shfl_sync(FULL, tt, 0);
+    if (tt < 0) break;
+    const int4 ti = ts.d_info[tt];
+    cut_tile<DIMS, TY, TZ, false>(ts.d_desc[ti.x], ti, tt, W, &ctr->cut_bad);
+    ++visits;
+    __syncwarp();
+    if (lane == 0) jfc::wl_done(W);
   }
   __shared__ unsigned long long s_vis;
   if (threadIdx.x == 0) s_vis = 0;
@@ -470,12 +284,357 @@ __global__ void __launch_bounds__(256) k_cut(const GridDev* __restrict__ gd,
   __syncthreads();
   if (threadIdx.x == 0) {
     if (s_vis) atomicAdd(&ctr->bfs_visits, s_vis);
-    __threadfence();
-    const unsigned prev = atomicAdd(&ctr->tk.done, 1u);
-    if (prev == gridDim.x - 1) {
-      ctr->tk.chunk = 0;
-      ctr->tk.done = 0;
-      __threadfence();
+    if (blockIdx.x == 0) {
+      ctr->bfs_passes = 1;
+      if (ctr->bfs_status == 0) ctr->bfs_status = 1;
+    }
+  }
+}
+
+// ------------------------------------------------------------ global relabel
+// One CTA per tile, one thread per node (the reference's work-group layout,
+// graphcut_global_relabel.cl:50-124): heights of the tile plus a one-cell halo
+// in shared memory, in-place relaxation h = min(h, h(v) + 1) over residual
+// arcs until a round changes nothing (monotone, so reading a neighbour's old
+// or new value is equally valid).
+template <int DIMS, int TY_, int TZ_>
+struct RTile {
+  static constexpr int TY = TY_, TZ = TZ_;
+  static constexpr int R = TY * TZ, NT = 32 * R, K = DIMS == 2 ? 4 : 6;
+  static constexpr int HX = 34, HY = TY + 2, HZ = DIMS == 3 ? TZ + 2 : 1, HN = HX * HY * HZ;
+  static constexpr int NHY = 2 * TZ * 32, NHX = 2 * R, NHZ = DIMS == 3 ? 2 * TY * 32 : 0;
+  static constexpr int NHALO = NHY + NHX + NHZ;
+  __device__ static constexpr int hidx(int x, int y, int z) {
+    return ((DIMS == 3 ? (z + 1) * HY : 0) + (y + 1)) * HX + (x + 1);
+  }
+};
+
+template <int DIMS, int TY, int TZ>
+struct RlSmem {
+  int h[RTile<DIMS, TY, TZ>::HN];
+  int tiles[8];
+  int ntile;
+  int face[6];
+};
+
+template <int DIMS, int TY, int TZ>
+__device__ __forceinline__ void rl_halo_cell(int c, int& x, int& y, int& z) {
+  using T = RTile<DIMS, TY, TZ>;
+  if (c < T::NHY) {
+    const int side = c / (TZ * 32), k = c % (TZ * 32);
+    x = k & 31; z = k >> 5; y = side ? TY : -1;
+  } else if (c < T::NHY + T::NHX) {
+    const int k = c - T::NHY, side = k / T::R, row = k % T::R;
+    x = side ? 32 : -1; y = row % TY; z = row / TY;
+  } else {
+    const int k = c - T::NHY - T::NHX, side = k / (TY * 32), m = k % (TY * 32);
+    x = m & 31; y = m >> 5; z = side ? TZ : -1;
+  }
+}
+
+template <int DIMS, int TY, int TZ, bool FIRST>
+__device__ __forceinline__ bool relabel_visit(const TileSet& ts, int tid, RlSmem<DIMS, TY, TZ>& s,
+                                              const BfsQ& Q, int& cur_grid, int& delta) {
+  using T = RTile<DIMS, TY, TZ>;
+  using D = Dirs<DIMS>;
+  const int t = threadIdx.x;
+  const int x = t & 31, row = t >> 5, y = row % TY, z = row / TY;
+  const int4 ti = ts.d_info[tid];
+  const GridDev& g = ts.d_desc[ti.x];
+  const int pitch = g.pitch;
+  const long long slab = (long long)g.pitch * g.Hp;
+  const int x0 = ti.y * 32, y0 = ti.z * TY, z0 = ti.w * TZ;
+  const long long tbase = (long long)x0 + (long long)y0 * pitch + (long long)z0 * slab;
+  const long long n = tbase + x + (long long)y * pitch + (long long)z * slab;
+  const int hi = T::hidx(x, y, z);
+  const int e = g.e[n];
+  unsigned arcs = 0;
+  arcs |= g.r[D::XP][n] > 0 ? 1u : 0u;
+  arcs |= g.r[D::YP][n] > 0 ? 2u : 0u;
+  arcs |= g.r[D::YM][n] > 0 ? 4u : 0u;
+  arcs |= g.r[D::XM][n] > 0 ? 8u : 0u;
+  if constexpr (DIMS == 3) {
+    arcs |= g.r[D::ZP][n] > 0 ? 16u : 0u;
+    arcs |= g.r[D::ZM][n] > 0 ? 32u : 0u;
+  }
+  const int hstart = FIRST ? (e < 0 ? 0 : JFC_INF) : g.h[n];
+  s.h[hi] = hstart;
+  for (int c = t; c < T::NHALO; c += T::NT) {
+    int hx, hy, hz;
+    rl_halo_cell<DIMS, TY, TZ>(c, hx, hy, hz);
+    const int gx = x0 + hx, gy = y0 + hy, gz = z0 + hz;
+    int v = JFC_INF;
+    if (gx >= 0 && gx < pitch && gy >= 0 && gy < g.Hp && gz >= 0 && gz < g.Dp) {
+      const long long m = (long long)gx + (long long)gy * pitch + (long long)gz * slab;
+      v = FIRST ? (g.e[m] < 0 ? 0 : JFC_INF) : g.h[m];
+    }
+    s.h[T::hidx(hx, hy, hz)] = v;
+  }
+  if (t < 6) s.face[t] = 0;
+  __syncthreads();
+  bool converged = false;
+  const int cap = 2 * (32 + TY + TZ);
+  for (int it = 0; it < cap; ++it) {
+    const int v = s.h[hi];
+    int m = v;
+    if (arcs & 1u) m = min(m, s.h[hi + 1] + 1);
+    if (arcs & 2u) m = min(m, s.h[hi + T::HX] + 1);
+    if (arcs & 4u) m = min(m, s.h[hi - T::HX] + 1);
+    if (arcs & 8u) m = min(m, s.h[hi - 1] + 1);
+    if constexpr (DIMS == 3) {
+      if (arcs & 16u) m = min(m, s.h[hi + T::HX * T::HY] + 1);
+      if (arcs & 32u) m = min(m, s.h[hi - T::HX * T::HY] + 1);
+    }
+    const bool ch = m < v;
+    if (ch) s.h[hi] = m;
+    if (!__syncthreads_or(ch)) { converged = true; break; }
+  }
+  const int hf = s.h[hi];
+  const bool changed = hf != hstart;
+  if (FIRST || changed) g.h[n] = hf;
+  if (changed) {
+    if (x == 0) s.face[0] = 1;
+    if (x == 31) s.face[1] = 1;
+    if (y == 0) s.face[2] = 1;
+    if (y == TY - 1) s.face[3] = 1;
+    if (DIMS == 3 && z == 0) s.face[4] = 1;
+    if (DIMS == 3 && z == TZ - 1) s.face[5] = 1;
+  }
+  const bool act = __syncthreads_or((e > 0) & (hf < JFC_INF));
+  if (t < 32) {
+    const int txs = g.tiles_x, tys = g.tiles_y;
+    bool want = false;
+    int nb = tid;
+    switch (t) {
+      case 0: want = s.face[0] && x0 > 0; nb = tid - 1; break;
+      case 1: want = s.face[1] && x0 + 32 < pitch; nb = tid + 1; break;
+      case 2: want = s.face[2] && y0 > 0; nb = tid - txs; break;
+      case 3: want = s.face[3] && y0 + TY < g.Hp; nb = tid + txs; break;
+      case 4: want = DIMS == 3 && s.face[4] && z0 > 0; nb = tid - txs * tys; break;
+      case 5: want = DIMS == 3 && s.face[5] && z0 + TZ < g.Dp; nb = tid + txs * tys; break;
+      case 6: want = !converged; nb = tid; break;
+      default: break;
+    }
+    if (want) jfc::wl_push(Q, nb);
+    if (t == 0) {
+      const int old = FIRST ? 0 : (int)ts.d_act[tid];
+      ts.d_act[tid] = act ? 1 : 0;
+      if (ti.x != cur_grid) {
+        if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
+        delta = 0;
+        cur_grid = ti.x;
+      }
+      delta += (act ? 1 : 0) - old;
+    }
+  }
+  __syncthreads();
+  return true;
+}
+
+// First pass of the global relabel, one warp per tile: a bit-parallel BFS
+// from the deficit nodes.  Each tile row is a 32-bit word (bit = lane); the
+// level-d frontier expands through the residual-arc masks in a few word
+// operations per row, so a tile costs (levels x rows) word ops and no block
+// barrier.  Halo nodes count as sources only when they are deficits
+// (h = 0 in this pass); everything later passes refine.
+template <int DIMS, int TY, int TZ>
+__device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, const BfsQ& Q, int& cur_grid,
+                                                   int& delta) {
+  using D = Dirs<DIMS>;
+  constexpr int R = TY * TZ;
+  const int lane = threadIdx.x & 31;
+  const int4 ti = ts.d_info[tid];
+  const GridDev& g = ts.d_desc[ti.x];
+  const Addr a = make_addr<DIMS, TY, TZ>(g, ti, lane);
+  unsigned AXP[R], AXM[R], AYP[R], AYM[R], AZP[DIMS == 3 ? R : 1], AZM[DIMS == 3 ? R : 1];
+  unsigned DEF[R], POS[R], V[R], F[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const long long n = roff<TY>(a, i);
+    const int e = g.e[n];
+    AXP[i] = __ballot_sync(FULL, g.r[D::XP][n] > 0);
+    AXM[i] = __ballot_sync(FULL, g.r[D::XM][n] > 0);
+    AYP[i] = __ballot_sync(FULL, g.r[D::YP][n] > 0);
+    AYM[i] = __ballot_sync(FULL, g.r[D::YM][n] > 0);
+    if constexpr (DIMS == 3) {
+      AZP[i] = __ballot_sync(FULL, g.r[D::ZP][n] > 0);
+      AZM[i] = __ballot_sync(FULL, g.r[D::ZM][n] > 0);
+    }
+    DEF[i] = __ballot_sync(FULL, e < 0);
+    POS[i] = __ballot_sync(FULL, e > 0);
+    V[i] = DEF[i];
+    F[i] = DEF[i];
+  }
+  // level-1 seeds: nodes with a residual arc into a deficit halo node
+  unsigned S1[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) S1[i] = 0u;
+#pragma unroll
+  for (int z = 0; z < TZ; ++z) {
+    const long long n = roff<TY>(a, z * TY);
+    const bool t0 = a.has_yT && g.e[n - a.pitch] < 0;
+    const bool t1 = a.has_yB && g.e[n + (long long)TY * a.pitch] < 0;
+    S1[z * TY] |= __ballot_sync(FULL, t0) & AYM[z * TY];
+    S1[z * TY + TY - 1] |= __ballot_sync(FULL, t1) & AYP[z * TY + TY - 1];
+  }
+  if constexpr (DIMS == 3) {
+#pragma unroll
+    for (int y = 0; y < TY; ++y) {
+      const long long n = roff<TY>(a, y);
+      const bool t0 = a.has_zT && g.e[n - a.slab] < 0;
+      const bool t1 = a.has_zB && g.e[n + (long long)TZ * a.slab] < 0;
+      S1[y] |= __ballot_sync(FULL, t0) & AZM[y];
+      S1[(TZ - 1) * TY + y] |= __ballot_sync(FULL, t1) & AZP[(TZ - 1) * TY + y];
+    }
+  }
+  {
+    const int row = lane & 15;
+    const bool left = lane < 16;
+    bool sdef = false;
+    if (row < R && (left ? a.has_xL : a.has_xR)) {
+      const long long n = (long long)(left ? a.x0 - 1 : a.x0 + 32) +
+                          (long long)(a.y0 + row % TY) * a.pitch + (long long)(a.z0 + row / TY) * a.slab;
+      sdef = g.e[n] < 0;
+    }
+    const unsigned sb = __ballot_sync(FULL, sdef);
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      S1[i] |= ((sb >> i) & 1u) & AXM[i];
+      S1[i] |= (((sb >> (16 + i)) & 1u) << 31) & AXP[i];
+    }
+  }
+  int h[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) h[i] = ((DEF[i] >> lane) & 1u) ? 0 : JFC_INF;
+  // level-synchronous expansion: u reaches level d+1 through an arc to a level-d node
+  for (int d = 0; d < 32 * R; ++d) {
+    unsigned any = 0;
+    unsigned N[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int y = i % TY, z = i / TY;
+      unsigned m = ((F[i] >> 1) & AXP[i]) | ((F[i] << 1) & AXM[i]);
+      if (y < TY - 1) m |= F[(i + 1 < R) ? i + 1 : i] & AYP[i];
+      if (y > 0) m |= F[(i > 0) ? i - 1 : 0] & AYM[i];
+      if constexpr (DIMS == 3) {
+        if (z < TZ - 1) m |= F[(i + TY < R) ? i + TY : i] & AZP[i];
+        if (z > 0) m |= F[(i >= TY) ? i - TY : 0] & AZM[i];
+      }
+      if (d == 0) m |= S1[i];
+      N[i] = m & ~V[i];
+      any |= N[i];
+    }
+    if (!any) break;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      V[i] |= N[i];
+      F[i] = N[i];
+      if ((N[i] >> lane) & 1u) h[i] = d + 1;
+    }
+  }
+  unsigned rows_fin = 0, c0 = 0, c31 = 0, act = 0;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    g.h[roff<TY>(a, i)] = h[i];
+    const unsigned fin = V[i] & ~DEF[i];   // finite and above 0: news for the neighbours
+    if (fin) rows_fin |= 1u << i;
+    c0 |= fin & 1u;
+    c31 |= fin >> 31;
+    act |= POS[i] & V[i];
+  }
+  if (lane == 0) {
+    const int old = 0;
+    ts.d_act[tid] = act ? 1 : 0;
+    if (ti.x != cur_grid) {
+      if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
+      delta = 0;
+      cur_grid = ti.x;
+    }
+    delta += (act ? 1 : 0) - old;
+  }
+  flag_neighbours<DIMS, TY, TZ>(g, a, tid, rows_fin, c0 != 0, c31 != 0, false, Q);
+}
+
+// Persistent global relabel: pass 0 initialises and relaxes every tile
+// (chunks of 8 tiles per ticket), later passes drain the frontier, then the
+// push-relabel queues are refilled with every tile holding an active node
+// (the reference's graphcut_count_node + clogs scan + graphcut_scatter_node,
+// graphcut_count_block.cl:19-65, as one warp-aggregated append).
+template <int DIMS, int TY, int TZ>
+__global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts, int max_passes) {
+  __shared__ RlSmem<DIMS, TY, TZ> sm;
+  DevCounters* ctr = ts.d_ctr;
+  const int lane = threadIdx.x & 31;
+  unsigned long long visits = 0;
+  int cur_grid = -1, delta = 0;
+  bool ok = true;
+  int pass = 0;
+  (void)max_passes;
+  const BfsQ W{ts.d_wq, ts.wq_cap, ts.d_flag_bfs[0], ctr};
+  {
+    // pass 0: one warp per tile (bit-parallel BFS), chunks of 8 tiles per ticket
+    int wgrid = -1, wdelta = 0;
+    for (;;) {
+      const unsigned c = jfc::warp_ticket(&ctr->ticket[0]);
+      const long long b = (long long)c * 8;
+      if (b >= ts.ntiles) break;
+      const int cnt = (int)min(8ll, (long long)ts.ntiles - b);
+      for (int k = 0; k < cnt; ++k) {
+        relabel_first_warp<DIMS, TY, TZ>(ts, (int)b + k, W, wgrid, wdelta);
+        ++visits;
+      }
+    }
+    if (lane == 0 && wdelta && wgrid >= 0) atomicAdd(&ts.d_grid_active[wgrid], wdelta);
+    ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
+  }
+  // then CTAs drain the work list, one tile per CTA
+  while (ok) {
+    if (threadIdx.x == 0) sm.ntile = jfc::wl_pop(W);
+    __syncthreads();
+    const int tt = sm.ntile;
+    __syncthreads();
+    if (tt < 0) break;
+    relabel_visit<DIMS, TY, TZ, false>(ts, tt, sm, W, cur_grid, delta);
+    if (threadIdx.x < 32) ++visits;
+    if (threadIdx.x == 0) jfc::wl_done(W);
+  }
+  pass = 1;
+  if (threadIdx.x == 0 && delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
+  // refill the push-relabel queues (buffer 0 of each parity) from the
+  // active-tile flags
+  if (ok) ok = jfc::grid_sync(ctr, [&]() {
+    ctr->qn_pr[0][0] = ctr->qn_pr[0][1] = ctr->qn_pr[1][0] = ctr->qn_pr[1][1] = 0;
+    ctr->cur_pr[0] = ctr->cur_pr[1] = 0;
+  });
+  if (ok) {
+    for (;;) {
+      const unsigned c = jfc::warp_ticket(&ctr->ticket[0]);
+      const long long b = (long long)c * 32;
+      if (b >= ts.ntiles) break;
+      const long long t = b + lane;
+      bool act = false;
+      int par = 0;
+      if (t < ts.ntiles) {
+        act = ts.d_act[t] != 0;
+        ts.d_flag_pr[t] = act ? 1 : 0;
+        if (act) { const int4 ti = ts.d_info[t]; par = (ti.y + ti.z + ti.w) & 1; }
+      }
+      jfc::warp_append(act && par == 0, (int)t, nullptr, ts.d_q_pr[0][0], &ctr->qn_pr[0][0]);
+      jfc::warp_append(act && par == 1, (int)t, nullptr, ts.d_q_pr[1][0], &ctr->qn_pr[1][0]);
+    }
+    ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
+  }
+  // pass-0 visits were counted per warp (lane 0 of each), later ones per block (thread 0)
+  __shared__ unsigned long long s_vis;
+  if (threadIdx.x == 0) s_vis = 0;
+  __syncthreads();
+  if (lane == 0 && visits) atomicAdd(&s_vis, visits);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_vis) atomicAdd(&ctr->bfs_visits, s_vis);
+    if (blockIdx.x == 0) {
+      ctr->bfs_passes = pass;
+      if (ctr->bfs_status == 0) ctr->bfs_status = 1;
     }
   }
 }
@@ -520,40 +679,16 @@ __global__ void __launch_bounds__(256) k_grid_sums(const GridDev* __restrict__ g
   }
 }
 
-template <int DIMS, int TY, int TZ>
-cudaError_t relabel_t(const TileSet& ts, int pass, bool first, cudaStream_t s) {
-  static int blocks_first = 0, blocks = 0;
-  uint8_t* fcur = ts.d_flag_bfs[pass & 1];
-  uint8_t* fnext = ts.d_flag_bfs[(pass + 1) & 1];
-  if (first) {
-    if (!blocks_first) blocks_first = persistent_blocks((const void*)k_relabel<DIMS, TY, TZ, true>, 256, 0);
-    jfc_note_launch();
-    k_relabel<DIMS, TY, TZ, true><<<blocks_first, 256, 0, s>>>(ts.d_desc, ts.d_info, ts.ntiles, fcur, fnext,
-                                                              ts.d_flag_pr, ts.d_grid_active, ts.d_ctr, pass);
-  } else {
-    if (!blocks) blocks = persistent_blocks((const void*)k_relabel<DIMS, TY, TZ, false>, 256, 0);
-    jfc_note_launch();
-    k_relabel<DIMS, TY, TZ, false><<<blocks, 256, 0, s>>>(ts.d_desc, ts.d_info, ts.ntiles, fcur, fnext,
-                                                         ts.d_flag_pr, ts.d_grid_active, ts.d_ctr, pass);
-  }
-  return cudaGetLastError();
-}
-
-template <int DIMS, int TY, int TZ>
-cudaError_t cut_t(const TileSet& ts, int pass, bool first, cudaStream_t s) {
-  static int blocks_first = 0, blocks = 0;
-  uint8_t* fcur = ts.d_flag_bfs[pass & 1];
-  uint8_t* fnext = ts.d_flag_bfs[(pass + 1) & 1];
-  if (first) {
-    if (!blocks_first) blocks_first = persistent_blocks((const void*)k_cut<DIMS, TY, TZ, true>, 256, 0);
-    jfc_note_launch();
-    k_cut<DIMS, TY, TZ, true><<<blocks_first, 256, 0, s>>>(ts.d_desc, ts.d_info, ts.ntiles, fcur, fnext, ts.d_ctr, pass);
-  } else {
-    if (!blocks) blocks = persistent_blocks((const void*)k_cut<DIMS, TY, TZ, false>, 256, 0);
-    jfc_note_launch();
-    k_cut<DIMS, TY, TZ, false><<<blocks, 256, 0, s>>>(ts.d_desc, ts.d_info, ts.ntiles, fcur, fnext, ts.d_ctr, pass);
-  }
-  return cudaGetLastError();
+template <int DIMS, int TY, int TZ, bool CUT>
+cudaError_t bfs_t(const TileSet& ts, int max_passes, cudaStream_t s) {
+  const void* fn = CUT ? (const void*)k_cut<DIMS, TY, TZ> : (const void*)k_relabel<DIMS, TY, TZ>;
+  const int nt = CUT ? 256 : RTile<DIMS, TY, TZ>::NT;
+  static int blocks = 0;
+  if (!blocks) blocks = persistent_blocks(fn, nt, 0);
+  TileSet arg = ts;
+  void* params[] = {(void*)&arg, (void*)&max_passes};
+  jfc_note_launch();
+  return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(nt), params, 0, s);
 }
 
 template <int TY, int TZ>
@@ -639,6 +774,19 @@ __global__ void k_edit_tlinks(GridDev g, const uint32_t* __restrict__ idx, const
 
 }  // namespace
 
+static int grid_blocks(long long n) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+// Work-list ring: cell i starts free for position i.
+__global__ void k_wq_init(unsigned long long* cells, unsigned cap) {
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x)
+    cells[i] = (unsigned long long)i << 32;
+}
+
 int persistent_blocks(const void* kernel, int threads, size_t smem) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
@@ -648,25 +796,16 @@ int persistent_blocks(const void* kernel, int threads, size_t smem) {
   return sms * per;
 }
 
-cudaError_t launch_relabel_pass(const TileSet& ts, int pass, bool first, cudaStream_t s) {
+cudaError_t launch_bfs(const TileSet& ts, bool cut, int max_passes, cudaStream_t s) {
+#define JFC_BFS(D, Y, Z) (cut ? bfs_t<D, Y, Z, true>(ts, max_passes, s) : bfs_t<D, Y, Z, false>(ts, max_passes, s))
   if (ts.dims == 2) {
-    if (ts.TR == 8) return relabel_t<2, 8, 1>(ts, pass, first, s);
-    if (ts.TR == 16) return relabel_t<2, 16, 1>(ts, pass, first, s);
+    if (ts.TR == 8) return JFC_BFS(2, 8, 1);
+    if (ts.TR == 16) return JFC_BFS(2, 16, 1);
     return cudaErrorInvalidValue;
   }
-  if (ts.TY == 4 && ts.TZ == 4) return relabel_t<3, 4, 4>(ts, pass, first, s);
-  if (ts.TY == 4 && ts.TZ == 2) return relabel_t<3, 4, 2>(ts, pass, first, s);
-  return cudaErrorInvalidValue;
-}
-
-cudaError_t launch_cut_pass(const TileSet& ts, int pass, bool first, cudaStream_t s) {
-  if (ts.dims == 2) {
-    if (ts.TR == 8) return cut_t<2, 8, 1>(ts, pass, first, s);
-    if (ts.TR == 16) return cut_t<2, 16, 1>(ts, pass, first, s);
-    return cudaErrorInvalidValue;
-  }
-  if (ts.TY == 4 && ts.TZ == 4) return cut_t<3, 4, 4>(ts, pass, first, s);
-  if (ts.TY == 4 && ts.TZ == 2) return cut_t<3, 4, 2>(ts, pass, first, s);
+  if (ts.TY == 4 && ts.TZ == 4) return JFC_BFS(3, 4, 4);
+  if (ts.TY == 4 && ts.TZ == 2) return JFC_BFS(3, 4, 2);
+#undef JFC_BFS
   return cudaErrorInvalidValue;
 }
 
@@ -684,14 +823,11 @@ cudaError_t launch_grid_sums(const TileSet& ts, cudaStream_t s) {
 }
 
 cudaError_t launch_clear_counters(const TileSet& ts, cudaStream_t s) {
-  return cudaMemsetAsync(ts.d_ctr, 0, sizeof(DevCounters), s);
-}
-
-static int grid_blocks(long long n) {
-  long long b = (n + 255) / 256;
-  if (b > 148 * 16) b = 148 * 16;
-  if (b < 1) b = 1;
-  return (int)b;
+  cudaError_t e = cudaMemsetAsync(ts.d_ctr, 0, sizeof(DevCounters), s);
+  if (e != cudaSuccess) return e;
+  jfc_note_launch();
+  k_wq_init<<<grid_blocks(ts.wq_cap), 256, 0, s>>>(ts.d_wq, ts.wq_cap);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_fix_boundary(const GridDev& g, int conn, int* d_bad, cudaStream_t s) {

@@ -363,6 +363,7 @@ int jfc_graph_create_grid(jfc_ctx* c, int dims, int w, int h, int d, int conn, j
   JFC_CUDA(cudaSetDevice(c->device));
   jfc_graph* G = new jfc_graph();
   G->ctx = c;
+  G->device = c->device;
   G->dims = dims; G->W = w; G->H = h; G->D = d; G->conn = conn;
   int pitch, Hp, Dp;
   grid_layout(dims, w, h, d, pitch, Hp, Dp);
@@ -389,8 +390,9 @@ int jfc_graph_create_grid(jfc_ctx* c, int dims, int w, int h, int d, int conn, j
 
 void jfc_graph_destroy(jfc_graph* G) {
   if (!G) return;
-  cudaSetDevice(G->ctx->device);
-  cudaStreamSynchronize(G->ctx->stream);
+  // the context may already be gone: use only what the graph owns
+  cudaSetDevice(G->device);
+  cudaDeviceSynchronize();
   tileset_free(G->ts);
   if (G->d_state) cudaFree(G->d_state);
   if (G->model.d_img) cudaFree(G->model.d_img);

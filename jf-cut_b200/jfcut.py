@@ -10,6 +10,7 @@ the library is missing or no GPU is present the call raises.
 """
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -46,7 +47,7 @@ class Stats(ctypes.Structure):
                 ("bfs_passes", ctypes.c_int), ("tile_visits", ctypes.c_longlong), ("flow", ctypes.c_longlong),
                 ("source_nodes", ctypes.c_longlong), ("ms_total", ctypes.c_double), ("ms_build", ctypes.c_double),
                 ("ms_push_relabel", ctypes.c_double), ("ms_global_relabel", ctypes.c_double),
-                ("ms_cut", ctypes.c_double)]
+                ("ms_cut", ctypes.c_double), ("pr_rounds", ctypes.c_longlong), ("bfs_visits", ctypes.c_longlong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -173,6 +174,7 @@ class Context:
 
     def __init__(self, device=0, **params):
         self.handle = VP()
+        self._children = weakref.WeakSet()
         p = default_params(**params)
         _check(_lib().jfc_create(device, ctypes.byref(p), ctypes.byref(self.handle)), "jfc_create")
 
@@ -192,7 +194,10 @@ class Context:
         return p
 
     def close(self):
+        """Destroy the context; graphs, batches and servers made from it go first."""
         if self.handle:
+            for child in list(self._children):
+                child.close()
             _lib().jfc_destroy(self.handle)
             self.handle = VP()
 
@@ -220,6 +225,7 @@ class Graph:
         self.handle = VP()
         _check(_lib().jfc_graph_create_grid(ctx.handle, self.dims, self.w, self.h, self.d, self.conn,
                                             ctypes.byref(self.handle)), "jfc_graph_create_grid")
+        ctx._children.add(self)
 
     # -- build (slotModelClicked: computeCapacity + kmeans + computeExcessFlowLazy)
     def build_from_image(self, img, seeds, pixfmt, model=None):
@@ -318,6 +324,7 @@ class Batch:
         self.handle = VP()
         self.graphs = []
         _check(_lib().jfc_batch_create(ctx.handle, ctypes.byref(self.handle)), "jfc_batch_create")
+        ctx._children.add(self)
 
     def add(self, g):
         _check(_lib().jfc_batch_add(self.handle, g.handle), "jfc_batch_add")
@@ -358,6 +365,7 @@ class Server:
         self.handle = VP()
         _check(_lib().jfc_server_create(ctx.handle, int(hbm_budget_bytes), int(max_slots),
                                         ctypes.byref(self.handle)), "jfc_server_create")
+        ctx._children.add(self)
 
     def submit(self, img, seeds, pixfmt, model=None):
         img = np.ascontiguousarray(img)

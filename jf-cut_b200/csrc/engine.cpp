@@ -112,9 +112,6 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDe
   const size_t o_fb1 = take(sizeof(int) * nt);
   const size_t o_qb0 = take(sizeof(int) * nt);
   const size_t o_qb1 = take(sizeof(int) * nt);
-  unsigned cap = 32;
-  while (cap < (unsigned)nt) cap <<= 1;
-  const size_t o_wq = take(sizeof(unsigned long long) * cap);
   const size_t o_act = take(nt);
   const size_t o_gact = take(sizeof(int) * grids.size());
   const size_t o_sum = take(sizeof(long long) * 2 * grids.size());
@@ -133,8 +130,6 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDe
   ts.d_q_bfs[0] = (int*)(blk + o_qb0);
   ts.d_q_bfs[1] = (int*)(blk + o_qb1);
   ts.d_act = (uint8_t*)(blk + o_act);
-  ts.d_wq = (unsigned long long*)(blk + o_wq);
-  ts.wq_cap = cap;
   ts.d_grid_active = (int*)(blk + o_gact);
   ts.d_grid_sum = (long long*)(blk + o_sum);
   ts.d_ctr = (DevCounters*)(blk + o_ctr);
@@ -241,6 +236,9 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
     st.ms_push_relabel += elapsed_ms(t_pr.a, t_pr.b);
     st.ms_global_relabel += elapsed_ms(t_gr.a, t_gr.b);
     ++st.global_relabels;
+    if (p.verbose)
+      fprintf(stderr, "{\"relabel\": %d, \"sweeps\": %d, \"active_tiles\": %lld, \"ms_pr\": %.3f, \"ms_gr\": %.3f}\n",
+              st.global_relabels, st.sweeps, total(), elapsed_ms(t_pr.a, t_pr.b), elapsed_ms(t_gr.a, t_gr.b));
   }
   if (status != JFC_OK) {
     for (int g = 0; g < ts.ngrids; ++g)

@@ -54,10 +54,6 @@ struct DevCounters {
   unsigned long long visits; // push-relabel tile visits
   unsigned long long bfs_visits;
   unsigned long long rounds; // push/relabel rounds summed over visits
-  unsigned wq_head;          // BFS work list: next cell to take
-  unsigned wq_tail;          // BFS work list: next cell to fill
-  int wq_pending;            // work items pushed and not yet finished
-  int pad2_;
 };
 
 // A set of grids tiled with one tile shape: the unit every launch works on
@@ -74,8 +70,6 @@ struct TileSet {
   int* d_q_pr[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [parity][buffer]
   int* d_flag_bfs[2] = {nullptr, nullptr};  // [buffer][ntiles] tile waits in a BFS frontier
   int* d_q_bfs[2] = {nullptr, nullptr};     // [buffer] BFS frontiers
-  unsigned long long* d_wq = nullptr;       // BFS work-list ring: (sequence << 32) | tile
-  unsigned wq_cap = 0;                      // ring size (power of two >= ntiles)
   uint8_t* d_act = nullptr;          // [ntiles] tile held an active node at its last relabel visit
   int* d_grid_active = nullptr;      // [ngrids] active tiles after global relabel
   long long* d_grid_sum = nullptr;   // [ngrids*2] sum min(e,0), source-side count
@@ -96,7 +90,7 @@ cudaError_t launch_pr_phase(const TileSet& ts, int sweeps, int local_iters, cuda
 // source-side cut (cut = true)
 cudaError_t launch_bfs(const TileSet& ts, bool cut, int max_passes, cudaStream_t s);
 cudaError_t launch_grid_sums(const TileSet& ts, cudaStream_t s);
-cudaError_t launch_clear_counters(const TileSet& ts, cudaStream_t s);  // also resets the work-list ring
+cudaError_t launch_clear_counters(const TileSet& ts, cudaStream_t s);
 int persistent_blocks(const void* kernel, int threads, size_t smem);
 // layout helpers (kernels_bfs.cu)
 cudaError_t launch_fix_boundary(const GridDev& g, int conn, int* d_bad, cudaStream_t s);

@@ -4,36 +4,37 @@
 // Global relabel — reference graphcut_init_global_relabel / graphcut_global_relabel
 // (graphcut_global_relabel.cl:19-124 2D, :128-249 3D) driven by QGCWidget::globalRelabel
 // (QGCWidget.cpp:2208-2241): heights = exact BFS distance to the deficit nodes
-// (e < 0) over residual arcs, computed by in-tile fixpoint relaxation
-// h = min(h, h(v) + 1) with tiles revisited in level sweeps ordered by the
-// jump-flooding tile BFS (graphcut_bfs_block.cl).
-// Here: the relaxation is monotone (heights only fall from INF), so every tile
-// may run at once with no parity and no ordering; a tile whose boundary fell
-// flags its neighbours in a double-buffered flag array and passes repeat until
-// no tile is flagged.  Each visit relaxes the whole warp tile in registers with
-// alternating top-down / bottom-up sweeps (lane = column, shuffles across
-// columns), which plays the role of the reference's in-tile fixpoint plus its
-// back-and-forth level order.  The first pass is fused with the initialisation
-// (h = 0 on deficits, INF elsewhere) and reads neighbour excess for its halo.
-// Each visit also records whether the tile holds an active node
-// (e > 0 and h < INF): this is the device-side active-tile count
-// (graphcut_count_node, graphcut_count_block.cl:19-47) that decides convergence.
+// (e < 0) over residual arcs, by in-tile fixpoint relaxation with tiles
+// revisited in level sweeps ordered by the jump-flooding tile BFS
+// (graphcut_bfs_block.cl).  Here the relaxation is monotone (heights only fall
+// from INF), so tiles need no parity and no order: a persistent cooperative
+// kernel runs a first pass over every tile (fused initialisation, one warp
+// per tile, bit-parallel level BFS) and then frontier passes (a tile whose
+// boundary fell queues its neighbours, grid barrier between passes) in which
+// one CTA per tile closes the in-tile distances with warp min-plus scans
+// along rows and columns.  Each visit records whether the tile holds an
+// active node (e > 0, h < INF): the device-side active-tile count
+// (graphcut_count_node, graphcut_count_block.cl:19-47) that decides
+// convergence, and the queue of tiles the next push-relabel phase visits.
 //
 // Cut — reference graphcut_init_cut / graphcut_compute_cut (graphcut_compute_cut.cl:19-140):
 // the source side is every node reachable from {e > 0} along residual arcs.
-// Here a warp tile is R rows of 32-bit words (bit = lane); each row's in-arc
-// masks are built once with ballots, propagation along a row is a 5-step
-// shift-doubling closure and across rows is word AND/OR, so a tile converges
-// in a few word operations per row.  Reaching a deficit raises cut_bad (the
-// reference's done[1] divergence flag).
-#include "jfc_sync.cuh"
+// One warp per tile: R rows of 32-bit words (bit = lane), in-arc masks built
+// once with ballots, row closure by 5-step shift doubling, rows combined by
+// word AND/OR.  Reaching a deficit raises cut_bad (the reference's done[1]
+// divergence flag).
+#include "jfc_relax.cuh"
 
 namespace {
 
 using jfc::FULL;
 
-// Work list the tile visits feed (deduplicated by its flags).
-using BfsQ = jfc::WorkList;
+// Frontier the tile visits feed (next pass), deduplicated by its flags.
+struct BfsQ {
+  int* flags;
+  int* q;
+  int* qn;
+};
 
 template <int DIMS>
 struct Dirs {
@@ -96,7 +97,7 @@ __device__ __forceinline__ void flag_neighbours(const GridDev& g, const Addr& a,
     case 6: want = again; nb = tid; break;
     default: break;
   }
-  if (want) jfc::wl_push(Q, nb);
+  jfc::warp_append(want, nb, Q.flags, Q.q, Q.qn);
 }
 
 // ------------------------------------------------------------------ cut BFS
@@ -244,38 +245,58 @@ __device__ __forceinline__ void cut_tile(const GridDev& g, int4 ti, int tid, con
   flag_neighbours<DIMS, TY, TZ>(g, a, tid, rows_changed, col0 != 0, col31 != 0, !converged, Q);
 }
 
-// Persistent cut BFS: the first pass visits every tile (labels start as
-// e > 0); then warps drain the work list (tiles whose halo labels changed),
-// one tile per warp, until nobody holds work and nothing is queued.
+// Persistent cut BFS: pass 0 visits every tile (labels start as e > 0),
+// later passes drain the frontier built by the previous one (one tile per
+// warp ticket), grid barriers in between, until a pass queues nothing or the
+// pass budget runs out.
 template <int DIMS, int TY, int TZ>
 __global__ void __launch_bounds__(256) k_cut(TileSet ts, int max_passes) {
   DevCounters* ctr = ts.d_ctr;
   const int lane = threadIdx.x & 31;
   unsigned long long visits = 0;
-  const BfsQ W{ts.d_wq, ts.wq_cap, ts.d_flag_bfs[0], ctr};
-  for (;;) {
-    const unsigned c = jfc::warp_ticket(&ctr->ticket[0]);
-    const long long b = (long long)c * 32;
-    if (b >= ts.ntiles) break;
-    const int cnt = (int)min(32ll, (long long)ts.ntiles - b);
-    for (int k = 0; k < cnt; ++k) {
-      const int tt = (int)b + k;
+  bool ok = true;
+  int pass = 0;
+  {
+    BfsQ Q{ts.d_flag_bfs[1], ts.d_q_bfs[1], &ctr->qn_bfs[1]};
+    for (;;) {
+      const unsigned c = jfc::warp_ticket(&ctr->ticket[0]);
+      const long long b = (long long)c * 32;
+      if (b >= ts.ntiles) break;
+      const int cnt = (int)min(32ll, (long long)ts.ntiles - b);
+      for (int k = 0; k < cnt; ++k) {
+        const int tt = (int)b + k;
+        const int4 ti = ts.d_info[tt];
+        cut_tile<DIMS, TY, TZ, true>(ts.d_desc[ti.x], ti, tt, Q, &ctr->cut_bad);
+        ++visits;
+      }
+    }
+    ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
+  }
+  for (pass = 1; ok; ++pass) {
+    const int cb = pass & 1;
+    const int n = jfc::vload(&ctr->qn_bfs[cb]);
+    if (n == 0) break;
+    if (pass > max_passes) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) ctr->bfs_status = 2;
+      break;
+    }
+    BfsQ Q{ts.d_flag_bfs[cb ^ 1], ts.d_q_bfs[cb ^ 1], &ctr->qn_bfs[cb ^ 1]};
+    const int* queue = ts.d_q_bfs[cb];
+    int* fcur = ts.d_flag_bfs[cb];
+    for (;;) {
+      const unsigned k = jfc::warp_ticket(&ctr->ticket[cb]);
+      if ((int)k >= n) break;
+      const int tt = queue[k];
+      if (lane == 0) fcur[tt] = 0;
+      __syncwarp();
       const int4 ti = ts.d_info[tt];
-      cut_tile<DIMS, TY, TZ, true>(ts.d_desc[ti.x], ti, tt, W, &ctr->cut_bad);
+      cut_tile<DIMS, TY, TZ, false>(ts.d_desc[ti.x], ti, tt, Q, &ctr->cut_bad);
       ++visits;
     }
-  }
-  bool ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
-  while (ok) {
-    int tt = 0;
-    if (lane == 0) tt = jfc::wl_pop(W);
-    tt = __shfl_sync(FULL, tt, 0);
-    if (tt < 0) break;
-    const int4 ti = ts.d_info[tt];
-    cut_tile<DIMS, TY, TZ, false>(ts.d_desc[ti.x], ti, tt, W, &ctr->cut_bad);
-    ++visits;
-    __syncwarp();
-    if (lane == 0) jfc::wl_done(W);
+    ok = jfc::grid_sync(ctr, [&]() {
+      ctr->ticket[cb] = 0;
+      ctr->qn_bfs[cb] = 0;
+    });
   }
   __shared__ unsigned long long s_vis;
   if (threadIdx.x == 0) s_vis = 0;
@@ -285,55 +306,31 @@ __global__ void __launch_bounds__(256) k_cut(TileSet ts, int max_passes) {
   if (threadIdx.x == 0) {
     if (s_vis) atomicAdd(&ctr->bfs_visits, s_vis);
     if (blockIdx.x == 0) {
-      ctr->bfs_passes = 1;
+      ctr->bfs_passes = pass;
       if (ctr->bfs_status == 0) ctr->bfs_status = 1;
     }
   }
 }
 
 // ------------------------------------------------------------ global relabel
-// One CTA per tile, one thread per node (the reference's work-group layout,
-// graphcut_global_relabel.cl:50-124): heights of the tile plus a one-cell halo
-// in shared memory, in-place relaxation h = min(h, h(v) + 1) over residual
-// arcs until a round changes nothing (monotone, so reading a neighbour's old
-// or new value is equally valid).
-template <int DIMS, int TY_, int TZ_>
-struct RTile {
-  static constexpr int TY = TY_, TZ = TZ_;
-  static constexpr int R = TY * TZ, NT = 32 * R, K = DIMS == 2 ? 4 : 6;
-  static constexpr int HX = 34, HY = TY + 2, HZ = DIMS == 3 ? TZ + 2 : 1, HN = HX * HY * HZ;
-  static constexpr int NHY = 2 * TZ * 32, NHX = 2 * R, NHZ = DIMS == 3 ? 2 * TY * 32 : 0;
-  static constexpr int NHALO = NHY + NHX + NHZ;
-  __device__ static constexpr int hidx(int x, int y, int z) {
-    return ((DIMS == 3 ? (z + 1) * HY : 0) + (y + 1)) * HX + (x + 1);
-  }
-};
+template <int DIMS, int TY, int TZ>
+using RTile = jfc::CtaTile<DIMS, TY, TZ>;
 
 template <int DIMS, int TY, int TZ>
 struct RlSmem {
   int h[RTile<DIMS, TY, TZ>::HN];
-  int tiles[8];
+  uint8_t arc[RTile<DIMS, TY, TZ>::NT];
   int ntile;
   int face[6];
 };
 
+// One frontier visit, one CTA per tile, one thread per node (the reference's
+// work-group layout, graphcut_global_relabel.cl:50-124): stage the tile's
+// heights and the halo, close the in-tile distances (relax_cta), write the
+// heights that fell, queue the neighbours whose halo fell and the tile itself
+// when its fixpoint was not reached.
 template <int DIMS, int TY, int TZ>
-__device__ __forceinline__ void rl_halo_cell(int c, int& x, int& y, int& z) {
-  using T = RTile<DIMS, TY, TZ>;
-  if (c < T::NHY) {
-    const int side = c / (TZ * 32), k = c % (TZ * 32);
-    x = k & 31; z = k >> 5; y = side ? TY : -1;
-  } else if (c < T::NHY + T::NHX) {
-    const int k = c - T::NHY, side = k / T::R, row = k % T::R;
-    x = side ? 32 : -1; y = row % TY; z = row / TY;
-  } else {
-    const int k = c - T::NHY - T::NHX, side = k / (TY * 32), m = k % (TY * 32);
-    x = m & 31; y = m >> 5; z = side ? TZ : -1;
-  }
-}
-
-template <int DIMS, int TY, int TZ, bool FIRST>
-__device__ __forceinline__ bool relabel_visit(const TileSet& ts, int tid, RlSmem<DIMS, TY, TZ>& s,
+__device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem<DIMS, TY, TZ>& s,
                                               const BfsQ& Q, int& cur_grid, int& delta) {
   using T = RTile<DIMS, TY, TZ>;
   using D = Dirs<DIMS>;
@@ -349,50 +346,33 @@ __device__ __forceinline__ bool relabel_visit(const TileSet& ts, int tid, RlSmem
   const int hi = T::hidx(x, y, z);
   const int e = g.e[n];
   unsigned arcs = 0;
-  arcs |= g.r[D::XP][n] > 0 ? 1u : 0u;
-  arcs |= g.r[D::YP][n] > 0 ? 2u : 0u;
-  arcs |= g.r[D::YM][n] > 0 ? 4u : 0u;
-  arcs |= g.r[D::XM][n] > 0 ? 8u : 0u;
+  arcs |= g.r[D::XP][n] > 0 ? jfc::A_XP : 0u;
+  arcs |= g.r[D::YP][n] > 0 ? jfc::A_YP : 0u;
+  arcs |= g.r[D::YM][n] > 0 ? jfc::A_YM : 0u;
+  arcs |= g.r[D::XM][n] > 0 ? jfc::A_XM : 0u;
   if constexpr (DIMS == 3) {
-    arcs |= g.r[D::ZP][n] > 0 ? 16u : 0u;
-    arcs |= g.r[D::ZM][n] > 0 ? 32u : 0u;
+    arcs |= g.r[D::ZP][n] > 0 ? jfc::A_ZP : 0u;
+    arcs |= g.r[D::ZM][n] > 0 ? jfc::A_ZM : 0u;
   }
-  const int hstart = FIRST ? (e < 0 ? 0 : JFC_INF) : g.h[n];
+  s.arc[t] = (uint8_t)arcs;
+  const int hstart = g.h[n];
   s.h[hi] = hstart;
   for (int c = t; c < T::NHALO; c += T::NT) {
-    int hx, hy, hz;
-    rl_halo_cell<DIMS, TY, TZ>(c, hx, hy, hz);
+    int hx, hy, hz, f;
+    T::halo_cell(c, hx, hy, hz, f);
     const int gx = x0 + hx, gy = y0 + hy, gz = z0 + hz;
     int v = JFC_INF;
-    if (gx >= 0 && gx < pitch && gy >= 0 && gy < g.Hp && gz >= 0 && gz < g.Dp) {
-      const long long m = (long long)gx + (long long)gy * pitch + (long long)gz * slab;
-      v = FIRST ? (g.e[m] < 0 ? 0 : JFC_INF) : g.h[m];
-    }
+    if (gx >= 0 && gx < pitch && gy >= 0 && gy < g.Hp && gz >= 0 && gz < g.Dp)
+      v = g.h[(long long)gx + (long long)gy * pitch + (long long)gz * slab];
     s.h[T::hidx(hx, hy, hz)] = v;
   }
   if (t < 6) s.face[t] = 0;
   __syncthreads();
-  bool converged = false;
-  const int cap = 2 * (32 + TY + TZ);
-  for (int it = 0; it < cap; ++it) {
-    const int v = s.h[hi];
-    int m = v;
-    if (arcs & 1u) m = min(m, s.h[hi + 1] + 1);
-    if (arcs & 2u) m = min(m, s.h[hi + T::HX] + 1);
-    if (arcs & 4u) m = min(m, s.h[hi - T::HX] + 1);
-    if (arcs & 8u) m = min(m, s.h[hi - 1] + 1);
-    if constexpr (DIMS == 3) {
-      if (arcs & 16u) m = min(m, s.h[hi + T::HX * T::HY] + 1);
-      if (arcs & 32u) m = min(m, s.h[hi - T::HX * T::HY] + 1);
-    }
-    const bool ch = m < v;
-    if (ch) s.h[hi] = m;
-    if (!__syncthreads_or(ch)) { converged = true; break; }
-  }
+  const bool converged = jfc::relax_cta<DIMS, TY, TZ>(s.h, s.arc, 16);
   const int hf = s.h[hi];
   const bool changed = hf != hstart;
-  if (FIRST || changed) g.h[n] = hf;
   if (changed) {
+    g.h[n] = hf;
     if (x == 0) s.face[0] = 1;
     if (x == 31) s.face[1] = 1;
     if (y == 0) s.face[2] = 1;
@@ -415,9 +395,9 @@ __device__ __forceinline__ bool relabel_visit(const TileSet& ts, int tid, RlSmem
       case 6: want = !converged; nb = tid; break;
       default: break;
     }
-    if (want) jfc::wl_push(Q, nb);
+    jfc::warp_append(want, nb, Q.flags, Q.q, Q.qn);
     if (t == 0) {
-      const int old = FIRST ? 0 : (int)ts.d_act[tid];
+      const int old = (int)ts.d_act[tid];
       ts.d_act[tid] = act ? 1 : 0;
       if (ti.x != cur_grid) {
         if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
@@ -428,7 +408,6 @@ __device__ __forceinline__ bool relabel_visit(const TileSet& ts, int tid, RlSmem
     }
   }
   __syncthreads();
-  return true;
 }
 
 // First pass of the global relabel, one warp per tile: a bit-parallel BFS
@@ -555,11 +534,12 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
   flag_neighbours<DIMS, TY, TZ>(g, a, tid, rows_fin, c0 != 0, c31 != 0, false, Q);
 }
 
-// Persistent global relabel: pass 0 initialises and relaxes every tile
-// (chunks of 8 tiles per ticket), later passes drain the frontier, then the
-// push-relabel queues are refilled with every tile holding an active node
-// (the reference's graphcut_count_node + clogs scan + graphcut_scatter_node,
-// graphcut_count_block.cl:19-65, as one warp-aggregated append).
+// Persistent global relabel: pass 0 initialises and closes every tile (one
+// warp per tile, chunks of 8 tiles per ticket), later passes drain the
+// frontier (one CTA per tile), then the push-relabel queues are refilled with
+// every tile holding an active node (the reference's graphcut_count_node +
+// clogs scan + graphcut_scatter_node, graphcut_count_block.cl:19-65, as one
+// warp-aggregated append).
 template <int DIMS, int TY, int TZ>
 __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts, int max_passes) {
   __shared__ RlSmem<DIMS, TY, TZ> sm;
@@ -569,10 +549,8 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts,
   int cur_grid = -1, delta = 0;
   bool ok = true;
   int pass = 0;
-  (void)max_passes;
-  const BfsQ W{ts.d_wq, ts.wq_cap, ts.d_flag_bfs[0], ctr};
   {
-    // pass 0: one warp per tile (bit-parallel BFS), chunks of 8 tiles per ticket
+    BfsQ Q{ts.d_flag_bfs[1], ts.d_q_bfs[1], &ctr->qn_bfs[1]};
     int wgrid = -1, wdelta = 0;
     for (;;) {
       const unsigned c = jfc::warp_ticket(&ctr->ticket[0]);
@@ -580,25 +558,42 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts,
       if (b >= ts.ntiles) break;
       const int cnt = (int)min(8ll, (long long)ts.ntiles - b);
       for (int k = 0; k < cnt; ++k) {
-        relabel_first_warp<DIMS, TY, TZ>(ts, (int)b + k, W, wgrid, wdelta);
+        relabel_first_warp<DIMS, TY, TZ>(ts, (int)b + k, Q, wgrid, wdelta);
         ++visits;
       }
     }
     if (lane == 0 && wdelta && wgrid >= 0) atomicAdd(&ts.d_grid_active[wgrid], wdelta);
     ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
   }
-  // then CTAs drain the work list, one tile per CTA
-  while (ok) {
-    if (threadIdx.x == 0) sm.ntile = jfc::wl_pop(W);
-    __syncthreads();
-    const int tt = sm.ntile;
-    __syncthreads();
-    if (tt < 0) break;
-    relabel_visit<DIMS, TY, TZ, false>(ts, tt, sm, W, cur_grid, delta);
-    if (threadIdx.x < 32) ++visits;
-    if (threadIdx.x == 0) jfc::wl_done(W);
+  for (pass = 1; ok; ++pass) {
+    const int cb = pass & 1;
+    const int n = jfc::vload(&ctr->qn_bfs[cb]);
+    if (n == 0) break;
+    if (pass > max_passes) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) ctr->bfs_status = 2;
+      break;
+    }
+    BfsQ Q{ts.d_flag_bfs[cb ^ 1], ts.d_q_bfs[cb ^ 1], &ctr->qn_bfs[cb ^ 1]};
+    const int* queue = ts.d_q_bfs[cb];
+    int* fcur = ts.d_flag_bfs[cb];
+    for (;;) {
+      if (threadIdx.x == 0) {
+        const unsigned k = atomicAdd(&ctr->ticket[cb], 1u);
+        sm.ntile = (int)k < n ? queue[k] : -1;
+        if ((int)k < n) fcur[sm.ntile] = 0;
+      }
+      __syncthreads();
+      const int tt = sm.ntile;
+      __syncthreads();
+      if (tt < 0) break;
+      relabel_visit<DIMS, TY, TZ>(ts, tt, sm, Q, cur_grid, delta);
+      if (threadIdx.x < 32) ++visits;
+    }
+    ok = jfc::grid_sync(ctr, [&]() {
+      ctr->ticket[cb] = 0;
+      ctr->qn_bfs[cb] = 0;
+    });
   }
-  pass = 1;
   if (threadIdx.x == 0 && delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
   // refill the push-relabel queues (buffer 0 of each parity) from the
   // active-tile flags
@@ -624,7 +619,7 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts,
     }
     ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
   }
-  // pass-0 visits were counted per warp (lane 0 of each), later ones per block (thread 0)
+  // pass-0 visits were counted per warp (lane 0 of each), later ones by warp 0
   __shared__ unsigned long long s_vis;
   if (threadIdx.x == 0) s_vis = 0;
   __syncthreads();
@@ -774,19 +769,6 @@ __global__ void k_edit_tlinks(GridDev g, const uint32_t* __restrict__ idx, const
 
 }  // namespace
 
-static int grid_blocks(long long n) {
-  long long b = (n + 255) / 256;
-  if (b > 148 * 16) b = 148 * 16;
-  if (b < 1) b = 1;
-  return (int)b;
-}
-
-// Work-list ring: cell i starts free for position i.
-__global__ void k_wq_init(unsigned long long* cells, unsigned cap) {
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x)
-    cells[i] = (unsigned long long)i << 32;
-}
-
 int persistent_blocks(const void* kernel, int threads, size_t smem) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
@@ -823,11 +805,14 @@ cudaError_t launch_grid_sums(const TileSet& ts, cudaStream_t s) {
 }
 
 cudaError_t launch_clear_counters(const TileSet& ts, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(ts.d_ctr, 0, sizeof(DevCounters), s);
-  if (e != cudaSuccess) return e;
-  jfc_note_launch();
-  k_wq_init<<<grid_blocks(ts.wq_cap), 256, 0, s>>>(ts.d_wq, ts.wq_cap);
-  return cudaGetLastError();
+  return cudaMemsetAsync(ts.d_ctr, 0, sizeof(DevCounters), s);
+}
+
+static int grid_blocks(long long n) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return (int)b;
 }
 
 cudaError_t launch_fix_boundary(const GridDev& g, int conn, int* d_bad, cudaStream_t s) {

@@ -26,31 +26,15 @@
 //    parity (deduplicated).  The phase stops early when both queues are empty.
 // Heights only grow between global relabels (relabel = 1 + min over residual
 // arcs, applied to active nodes without an admissible arc).
-#include "jfc_sync.cuh"
+#include "jfc_relax.cuh"
+
 
 namespace {
 
 using jfc::FULL;
 
-template <int DIMS, int TY_, int TZ_>
-struct Tile {
-  static constexpr int TY = TY_, TZ = TZ_;
-  static constexpr int R = TY * TZ;            // rows = warps
-  static constexpr int NT = 32 * R;            // threads = nodes
-  static constexpr int K = DIMS == 2 ? 4 : 6;  // arcs per node
-  static constexpr int HX = 34, HY = TY + 2, HZ = DIMS == 3 ? TZ + 2 : 1;
-  static constexpr int HN = HX * HY * HZ;      // height box with a one-cell halo
-  // arc slots (reference channel order)
-  static constexpr int XP = 0, YP = 1;
-  static constexpr int ZP = DIMS == 2 ? 0 : 2, ZM = DIMS == 2 ? 0 : 3;
-  static constexpr int YM = DIMS == 2 ? 2 : 4, XM = DIMS == 2 ? 3 : 5;
-  // halo cells: y faces (2 x TZ x 32), x faces (2 x R), z faces (2 x TY x 32)
-  static constexpr int NHY = 2 * TZ * 32, NHX = 2 * R, NHZ = DIMS == 3 ? 2 * TY * 32 : 0;
-  static constexpr int NHALO = NHY + NHX + NHZ;
-  __device__ static constexpr int hidx(int x, int y, int z) {
-    return ((DIMS == 3 ? (z + 1) * HY : 0) + (y + 1)) * HX + (x + 1);
-  }
-};
+template <int DIMS, int TY, int TZ>
+using Tile = jfc::CtaTile<DIMS, TY, TZ>;
 
 template <int DIMS, int TY, int TZ>
 struct PrSmem {
@@ -59,24 +43,14 @@ struct PrSmem {
   int h[T::HN];
   int r[T::K][T::NT];
   int out[T::NHALO];      // flow pushed into each halo cell during the visit
+  uint8_t arc[T::NT];     // residual-arc bits for the local relabel
   int tile;
   int face[6];            // any flow left through face: x-, x+, y-, y+, z-, z+
 };
 
-// Halo cell c -> (x, y, z) relative to the tile origin and the face it lies on.
 template <int DIMS, int TY, int TZ>
 __device__ __forceinline__ void halo_cell(int c, int& x, int& y, int& z, int& face) {
-  using T = Tile<DIMS, TY, TZ>;
-  if (c < T::NHY) {
-    const int side = c / (TZ * 32), k = c % (TZ * 32);
-    x = k & 31; z = k >> 5; y = side ? TY : -1; face = side ? 3 : 2;
-  } else if (c < T::NHY + T::NHX) {
-    const int k = c - T::NHY, side = k / T::R, row = k % T::R;
-    x = side ? 32 : -1; y = row % TY; z = row / TY; face = side ? 1 : 0;
-  } else {
-    const int k = c - T::NHY - T::NHX, side = k / (TY * 32), m = k % (TY * 32);
-    x = m & 31; y = m >> 5; z = side ? TZ : -1; face = side ? 5 : 4;
-  }
+  Tile<DIMS, TY, TZ>::halo_cell(c, x, y, z, face);
 }
 
 template <int DIMS, int TY, int TZ>
@@ -114,6 +88,31 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
     s.out[c] = 0;
   }
   if (t < 6) s.face[t] = 0;
+  {
+    unsigned a = 0;
+    a |= r0[T::XP] > 0 ? jfc::A_XP : 0u;
+    a |= r0[T::YP] > 0 ? jfc::A_YP : 0u;
+    a |= r0[T::YM] > 0 ? jfc::A_YM : 0u;
+    a |= r0[T::XM] > 0 ? jfc::A_XM : 0u;
+    if constexpr (DIMS == 3) {
+      a |= r0[T::ZP] > 0 ? jfc::A_ZP : 0u;
+      a |= r0[T::ZM] > 0 ? jfc::A_ZM : 0u;
+    }
+    s.arc[t] = (uint8_t)a;
+    // local relabel: distance to the nearest in-tile deficit or halo node
+    // over residual arcs (halo heights fixed), then h = max(h, distance).
+    // The pointwise max of two valid labellings is valid, so heights stay
+    // monotone (push-relabel termination holds) while excess trapped in the
+    // tile jumps straight to INF instead of climbing one level per round.
+    s.h[hi] = e0 < 0 ? 0 : JFC_INF;
+  }
+  __syncthreads();
+  {
+    // a partial relaxation overestimates distances, so the local labelling
+    // is only applied when the in-tile fixpoint was reached
+    const bool exact = jfc::relax_cta<DIMS, TY, TZ>(s.h, s.arc, 8);
+    s.h[hi] = exact ? max(s.h[hi], h0) : h0;
+  }
   __syncthreads();
 
   // in-tile neighbours, or the halo cell a push across the border lands in

@@ -183,6 +183,25 @@ int jfc_edit_tlinks(jfc_graph* g, const uint32_t* idx, const int32_t* dcs,
  * QGCWidget.cpp:2243-2287).  Duplicate indices: the last one wins. */
 int jfc_graph_edit_seeds(jfc_graph* g, const uint32_t* idx, const uint8_t* new_seed, size_t n);
 
+/* Solve a 2D 4-connected grid without allocating anything.  No counterpart in
+ * the reference: it exists for callers that cannot allocate device memory
+ * when they need a cut (code running during CUDA stream capture, real-time
+ * frame loops that must not stall on the allocator, hosts with a fixed memory
+ * budget).  The working set lives in one fixed file-scope device array of
+ * about 13.2 MB that every GPU loading the library holds until exit; grids
+ * are limited to 524,288 nodes after padding (width to a multiple of 32,
+ * height to a multiple of 16), larger ones return JFC_ERR_INVALID_ARG.
+ * Inputs d_excess and d_ncap[4] (reference channel order, dense w*h int32)
+ * and the output d_labels (w*h bytes, 1 = source side) are caller-owned
+ * device buffers on `device`; *flow receives the int64 max-flow.  stream is
+ * a cudaStream_t (NULL = the legacy default stream); params may be NULL.
+ * Calls share the array: calls that overlap on the GPU race.  The first call
+ * on a device looks up the array's address; make it before any stream
+ * capture begins. */
+int jfc_solve_grid2d_noalloc(int device, void* stream, const jfc_params* params, int w, int h,
+                             const int32_t* d_excess, const int32_t* const* d_ncap,
+                             int64_t flow_offset, uint8_t* d_labels, int64_t* flow);
+
 /* ---- batched solver: many independent grids in one persistent launch per
  * phase, fed by a device work queue (no reference counterpart; the reference
  * solves one volume at a time, QGCWidget.cpp:2364). ---- */

@@ -101,6 +101,9 @@ def _lib():
         L.jfc_read_labels_device.argtypes = [VP, VP]
         L.jfc_edit_tlinks.argtypes = [VP, U32P, I32P, I32P, ctypes.c_size_t]
         L.jfc_graph_edit_seeds.argtypes = [VP, U32P, U8P, ctypes.c_size_t]
+        L.jfc_solve_grid2d_noalloc.argtypes = [ctypes.c_int, VP, ctypes.POINTER(Params), ctypes.c_int,
+                                               ctypes.c_int, VP, ctypes.POINTER(VP), ctypes.c_int64, VP,
+                                               ctypes.POINTER(ctypes.c_int64)]
         L.jfc_batch_create.argtypes = [VP, ctypes.POINTER(VP)]
         L.jfc_batch_destroy.argtypes = [VP]
         L.jfc_batch_destroy.restype = None
@@ -314,6 +317,19 @@ class Graph:
             self.close()
         except Exception:
             pass
+
+
+def solve_grid2d_noalloc(w, h, d_excess, d_caps, d_labels, flow_offset=0, device=0, stream=0, params=None):
+    """2D solve that allocates nothing (fixed device working set, grids up to
+    524,288 padded nodes).  d_excess, d_caps[4], d_labels are device pointers
+    (ints); returns the int64 max-flow."""
+    P = (VP * 4)(*[VP(int(p)) for p in d_caps])
+    f = ctypes.c_int64()
+    _check(_lib().jfc_solve_grid2d_noalloc(int(device), VP(stream or None),
+                                           ctypes.byref(params) if params is not None else None,
+                                           int(w), int(h), VP(int(d_excess)), P, int(flow_offset),
+                                           VP(int(d_labels)), ctypes.byref(f)), "jfc_solve_grid2d_noalloc")
+    return f.value
 
 
 class Batch:

@@ -73,11 +73,13 @@ enum { JFC_SEED_NONE = 0, JFC_SEED_FG = 1, JFC_SEED_BG = 2 };
 typedef struct jfc_params {
   int tile_rows;         /* 2D warp-tile height: 8 or 16 (default 16); 3D uses 32x4x4 */
   int local_iters;       /* push/relabel rounds per tile visit (default 16) */
-  int relabel_interval;  /* parity sweeps between global relabels (default 8) */
+  int relabel_interval;  /* sweep pairs between global relabels at the start (default 4) */
   int max_sweeps;        /* budget of sweeps -> JFC_ERR_NOT_CONVERGED (default 1<<20) */
   int max_bfs_passes;    /* budget of tile passes per BFS (default 1<<20) */
-  int use_graph;         /* 1: capture the solve loop in a CUDA graph (default 1) */
-  int verbose;           /* 1: one JSON line per solve on stderr */
+  int use_graph;         /* reserved (0) */
+  int verbose;           /* 1: one JSON line per global relabel on stderr */
+  int relabel_interval_max; /* adaptive interval cap: the interval doubles while fewer
+                               than 1/256 of the tiles are active (default 16 x interval) */
 } jfc_params;
 
 /* Capacity model (replaces computeCapacity / kmeans / computeExcessFlowLazy,
@@ -107,6 +109,8 @@ typedef struct jfc_stats {
   double ms_total, ms_build, ms_push_relabel, ms_global_relabel, ms_cut;
   long long pr_rounds;    /* push/relabel rounds summed over tile visits */
   long long bfs_visits;   /* tile visits of all BFS passes */
+  double ms_gr_first;     /* global relabel: dense first passes (device clock) */
+  double ms_gr_frontier;  /* global relabel: frontier passes (device clock) */
 } jfc_stats;
 
 typedef struct jfc_ctx jfc_ctx;

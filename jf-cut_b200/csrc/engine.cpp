@@ -20,6 +20,7 @@
 // instead of returning a non-converged cut.
 #include "engine.h"
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -49,7 +50,8 @@ extern "C" const char* jfc_last_error(void) { return g_err.c_str(); }
 void fill_defaults(jfc_params& p) {
   if (p.tile_rows != 8 && p.tile_rows != 16) p.tile_rows = 16;
   if (p.local_iters <= 0) p.local_iters = 16;
-  if (p.relabel_interval <= 0) p.relabel_interval = 8;
+  if (p.relabel_interval <= 0) p.relabel_interval = 4;
+  if (p.relabel_interval_max < p.relabel_interval) p.relabel_interval_max = 16 * p.relabel_interval;
   if (p.max_sweeps <= 0) p.max_sweeps = 1 << 20;
   if (p.max_bfs_passes <= 0) p.max_bfs_passes = 1 << 20;
 }
@@ -217,6 +219,11 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
 
   auto total = [&]() { long long t = 0; for (int v : active) t += v; return t; };
   int status = JFC_OK;
+  // Adaptive schedule: while a large part of the grid is active, frequent
+  // global relabels pay off; once only a sliver is active (long transport
+  // paths, few tiles), the dense relabel dominates, so the interval doubles
+  // (the push-relabel phase still stops as soon as its queues drain).
+  int interval = p.relabel_interval;
   while (total() > 0) {
     if (st.sweeps >= p.max_sweeps) {
       status = set_error(JFC_ERR_NOT_CONVERGED, "sweep budget exhausted");
@@ -225,7 +232,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
     // relabel_interval x (even sweep, odd sweep) in one persistent launch
     JFC_CUDA(cudaEventRecord(t_pr.a, s));
     JFC_CUDA(cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s));
-    JFC_CUDA(launch_pr_phase(ts, p.relabel_interval, p.local_iters, s));
+    JFC_CUDA(launch_pr_phase(ts, interval, p.local_iters, s));
     JFC_CUDA(cudaEventRecord(t_pr.b, s));
     // global relabel + active-tile count (one host read-back per cycle)
     JFC_CUDA(cudaEventRecord(t_gr.a, s));
@@ -233,6 +240,8 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
     rc = run_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, t_gr.b, &sw);
     if (rc) return rc;
     st.sweeps += sw;
+    if (total() * 256 < (long long)ts.ntiles) interval = std::min(interval * 2, p.relabel_interval_max);
+    else interval = p.relabel_interval;
     st.ms_push_relabel += elapsed_ms(t_pr.a, t_pr.b);
     st.ms_global_relabel += elapsed_ms(t_gr.a, t_gr.b);
     ++st.global_relabels;
@@ -257,7 +266,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   long long* hs = (long long*)ctx->h_pin;
   unsigned long long* hv = (unsigned long long*)(hs + 2 * ts.ngrids);
   JFC_CUDA(cudaMemcpyAsync(hs, ts.d_grid_sum, sizeof(long long) * 2 * ts.ngrids, cudaMemcpyDeviceToHost, s));
-  JFC_CUDA(cudaMemcpyAsync(hv, &ts.d_ctr->visits, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  JFC_CUDA(cudaMemcpyAsync(hv, &ts.d_ctr->visits, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   JFC_CUDA(cudaEventRecord(t_all.b, s));
   JFC_CUDA(cudaStreamSynchronize(s));
   st.ms_cut = elapsed_ms(t_cut.a, t_cut.b);
@@ -265,6 +274,8 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   st.tile_visits = (long long)hv[0];
   st.bfs_visits = (long long)hv[1];
   st.pr_rounds = (long long)hv[2];
+  st.ms_gr_first = hv[3] * 1e-6;
+  st.ms_gr_frontier = hv[4] * 1e-6;
   for (int g = 0; g < ts.ngrids; ++g) {
     res[g].neg_sum = hs[2 * g];
     res[g].labels = hs[2 * g + 1];

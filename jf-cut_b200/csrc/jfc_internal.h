@@ -54,6 +54,8 @@ struct DevCounters {
   unsigned long long visits; // push-relabel tile visits
   unsigned long long bfs_visits;
   unsigned long long rounds; // push/relabel rounds summed over visits
+  unsigned long long ns_gr_first;     // global relabel: first (dense) pass, device ns
+  unsigned long long ns_gr_frontier;  // global relabel: frontier passes + queue refill
 };
 
 // A set of grids tiled with one tile shape: the unit every launch works on

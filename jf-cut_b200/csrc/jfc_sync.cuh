@@ -45,6 +45,13 @@ __device__ __forceinline__ bool grid_sync(DevCounters* ctr, F on_last) {
 
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
 
+// Device-wide nanosecond clock (phase timing of the persistent kernels).
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Warp-cooperative append of up to 32 candidate tiles: lane k offers `tile`
 // when `want`; with `flags`, a tile is appended only by the lane that flips
 // its flag 0 -> 1 (so a queue never holds a tile twice).

@@ -549,6 +549,8 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts,
   int cur_grid = -1, delta = 0;
   bool ok = true;
   int pass = 0;
+  const unsigned long long t0 = jfc::global_ns();
+  unsigned long long t1 = t0;
   {
     BfsQ Q{ts.d_flag_bfs[1], ts.d_q_bfs[1], &ctr->qn_bfs[1]};
     int wgrid = -1, wdelta = 0;
@@ -564,6 +566,7 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts,
     }
     if (lane == 0 && wdelta && wgrid >= 0) atomicAdd(&ts.d_grid_active[wgrid], wdelta);
     ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
+    t1 = jfc::global_ns();
   }
   for (pass = 1; ok; ++pass) {
     const int cb = pass & 1;
@@ -630,6 +633,9 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts,
     if (blockIdx.x == 0) {
       ctr->bfs_passes = pass;
       if (ctr->bfs_status == 0) ctr->bfs_status = 1;
+      const unsigned long long t2 = jfc::global_ns();
+      ctr->ns_gr_first += t1 - t0;
+      ctr->ns_gr_frontier += t2 - t1;
     }
   }
 }

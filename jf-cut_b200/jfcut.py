@@ -34,7 +34,7 @@ class JfcError(RuntimeError):
 
 class Params(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("tile_rows", "local_iters", "relabel_interval", "max_sweeps",
-                                             "max_bfs_passes", "use_graph", "verbose")]
+                                             "max_bfs_passes", "use_graph", "verbose", "relabel_interval_max")]
 
 
 class Model(ctypes.Structure):
@@ -47,7 +47,8 @@ class Stats(ctypes.Structure):
                 ("bfs_passes", ctypes.c_int), ("tile_visits", ctypes.c_longlong), ("flow", ctypes.c_longlong),
                 ("source_nodes", ctypes.c_longlong), ("ms_total", ctypes.c_double), ("ms_build", ctypes.c_double),
                 ("ms_push_relabel", ctypes.c_double), ("ms_global_relabel", ctypes.c_double),
-                ("ms_cut", ctypes.c_double), ("pr_rounds", ctypes.c_longlong), ("bfs_visits", ctypes.c_longlong)]
+                ("ms_cut", ctypes.c_double), ("pr_rounds", ctypes.c_longlong), ("bfs_visits", ctypes.c_longlong),
+                ("ms_gr_first", ctypes.c_double), ("ms_gr_frontier", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

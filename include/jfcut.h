@@ -243,6 +243,14 @@ int  jfc_server_wait(jfc_server* s, int sid, int timeout_ms, jfc_request_info* i
 int  jfc_server_read_labels(jfc_server* s, int sid, uint8_t* out);
 int  jfc_server_close(jfc_server* s, int sid);      /* frees the session's device state */
 int  jfc_server_cancel(jfc_server* s, int sid);
+/* Server counters: budget and bytes held (now / peak), sessions by phase, the
+ * largest solving set seen (grids sharing one launch), loop iterations. */
+typedef struct jfc_server_stats {
+  size_t budget, used, peak_used;
+  int sessions, waiting, solving, peak_solving;
+  int64_t loops, requests_done;
+} jfc_server_stats;
+int  jfc_server_get_stats(jfc_server* s, jfc_server_stats* out);
 
 /* ---- synthetic inputs (seeded, deterministic, integer arithmetic) used by the
  * tests and the benchmark in place of the reference's image files ---- */

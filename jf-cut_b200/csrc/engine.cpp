@@ -68,60 +68,31 @@ static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 void tileset_free(TileSet& ts) {
   if (ts.d_block) cudaFree(ts.d_block);
+  if (ts.h_stage) cudaFreeHost(ts.h_stage);
   ts = TileSet();
 }
 
-int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDev>& grids_in) {
-  tileset_free(ts);
-  ts.dims = dims;
-  if (dims == 2) {
-    ts.TR = tile_rows; ts.TY = tile_rows; ts.TZ = 1;
-  } else {
-    ts.TR = tile_rows; ts.TY = 4; ts.TZ = tile_rows >= 16 ? 4 : 2;
-  }
-  std::vector<GridDev> grids = grids_in;
-  std::vector<int4> info;
-  int base = 0, npar[2] = {0, 0};
-  for (size_t gi = 0; gi < grids.size(); ++gi) {
-    GridDev& g = grids[gi];
-    if (g.dims != dims) return set_error(JFC_ERR_INVALID_ARG, "tile set mixes 2D and 3D grids");
-    g.tiles_x = g.pitch / JFC_TW;
-    g.tiles_y = g.Hp / ts.TY;
-    g.tiles_z = g.Dp / ts.TZ;
-    g.tile_base = base;
-    for (int tz = 0; tz < g.tiles_z; ++tz)
-      for (int ty = 0; ty < g.tiles_y; ++ty)
-        for (int tx = 0; tx < g.tiles_x; ++tx) {
-          info.push_back(make_int4((int)gi, tx, ty, tz));
-          ++npar[(tx + ty + tz) & 1];
-        }
-    base += g.tiles_x * g.tiles_y * g.tiles_z;
-  }
-  ts.ngrids = (int)grids.size();
-  ts.ntiles = base;
-  ts.nlist[0] = npar[0];
-  ts.nlist[1] = npar[1];
-  const size_t nt = (size_t)ts.ntiles;
+// Carve the control block for cap_tiles tiles / cap_grids grids.
+static void tileset_carve(TileSet& ts, char* blk, size_t* total) {
+  const size_t nt = (size_t)ts.cap_tiles, ng = (size_t)ts.cap_grids;
   size_t off = 0;
   auto take = [&](size_t bytes) { const size_t o = off; off = align_up(off + bytes, 256); return o; };
-  const size_t o_desc = take(sizeof(GridDev) * grids.size());
+  const size_t o_desc = take(sizeof(GridDev) * ng);
   const size_t o_info = take(sizeof(int4) * nt);
   const size_t o_fpr = take(sizeof(int) * nt);
   size_t o_qpr[2][2];
   for (int p = 0; p < 2; ++p)
-    for (int b = 0; b < 2; ++b) o_qpr[p][b] = take(sizeof(int) * (size_t)npar[p]);
+    for (int b = 0; b < 2; ++b) o_qpr[p][b] = take(sizeof(int) * nt);
   const size_t o_fb0 = take(sizeof(int) * nt);
   const size_t o_fb1 = take(sizeof(int) * nt);
   const size_t o_qb0 = take(sizeof(int) * nt);
   const size_t o_qb1 = take(sizeof(int) * nt);
   const size_t o_act = take(nt);
-  const size_t o_gact = take(sizeof(int) * grids.size());
-  const size_t o_sum = take(sizeof(long long) * 2 * grids.size());
+  const size_t o_gact = take(sizeof(int) * ng);
+  const size_t o_sum = take(sizeof(long long) * 2 * ng);
   const size_t o_ctr = take(sizeof(DevCounters));
-  char* blk = nullptr;
-  JFC_CUDA(cudaMalloc((void**)&blk, off));
-  ts.d_block = blk;
-  ts.block_bytes = off;
+  *total = off;
+  if (!blk) return;
   ts.d_desc = (GridDev*)(blk + o_desc);
   ts.d_info = (int4*)(blk + o_info);
   ts.d_flag_pr = (int*)(blk + o_fpr);
@@ -135,9 +106,88 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDe
   ts.d_grid_active = (int*)(blk + o_gact);
   ts.d_grid_sum = (long long*)(blk + o_sum);
   ts.d_ctr = (DevCounters*)(blk + o_ctr);
-  JFC_CUDA(cudaMemset(blk, 0, off));
-  JFC_CUDA(cudaMemcpy(ts.d_desc, grids.data(), sizeof(GridDev) * grids.size(), cudaMemcpyHostToDevice));
-  JFC_CUDA(cudaMemcpy(ts.d_info, info.data(), sizeof(int4) * info.size(), cudaMemcpyHostToDevice));
+}
+
+int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDev>& grids_in, cudaStream_t s) {
+  int TY, TZ;
+  if (dims == 2) {
+    TY = tile_rows; TZ = 1;
+  } else {
+    TY = 4; TZ = tile_rows >= 16 ? 4 : 2;
+  }
+  std::vector<GridDev> grids = grids_in;
+  int base = 0, npar[2] = {0, 0};
+  for (size_t gi = 0; gi < grids.size(); ++gi) {
+    GridDev& g = grids[gi];
+    if (g.dims != dims) return set_error(JFC_ERR_INVALID_ARG, "tile set mixes 2D and 3D grids");
+    g.tiles_x = g.pitch / JFC_TW;
+    g.tiles_y = g.Hp / TY;
+    g.tiles_z = g.Dp / TZ;
+    g.tile_base = base;
+    base += g.tiles_x * g.tiles_y * g.tiles_z;
+  }
+  const int ntiles = base, ngrids = (int)grids.size();
+  // reuse the control block while it is large enough (the server re-forms its
+  // tile sets between relabels); otherwise allocate with headroom when asked
+  // to stage asynchronously
+  if (!ts.d_block || ts.cap_tiles < ntiles || ts.cap_grids < ngrids) {
+    tileset_free(ts);
+    ts.cap_tiles = s ? ntiles + ntiles / 4 + 64 : ntiles;
+    ts.cap_grids = s ? ngrids + ngrids / 4 + 8 : ngrids;
+    if (ts.cap_tiles < 1) ts.cap_tiles = 1;
+    if (ts.cap_grids < 1) ts.cap_grids = 1;
+    size_t total = 0;
+    tileset_carve(ts, nullptr, &total);
+    char* blk = nullptr;
+    JFC_CUDA(cudaMalloc((void**)&blk, total));
+    ts.d_block = blk;
+    ts.block_bytes = total;
+    tileset_carve(ts, blk, &total);
+    JFC_CUDA(cudaMemset(blk, 0, total));
+  }
+  ts.dims = dims;
+  ts.TR = tile_rows; ts.TY = TY; ts.TZ = TZ;
+  ts.ngrids = ngrids;
+  ts.ntiles = ntiles;
+  const size_t desc_bytes = sizeof(GridDev) * (size_t)ngrids, info_bytes = sizeof(int4) * (size_t)ntiles;
+  const size_t stage = align_up(desc_bytes, 256) + info_bytes;
+  int4* info;
+  if (s) {
+    if (ts.h_stage_bytes < stage) {
+      if (ts.h_stage) cudaFreeHost(ts.h_stage);
+      ts.h_stage = nullptr;
+      ts.h_stage_bytes = 0;
+      JFC_CUDA(cudaMallocHost(&ts.h_stage, stage + stage / 4));
+      ts.h_stage_bytes = stage + stage / 4;
+    }
+    std::memcpy(ts.h_stage, grids.data(), desc_bytes);
+    info = (int4*)((char*)ts.h_stage + align_up(desc_bytes, 256));
+  } else {
+    static thread_local std::vector<int4> v;
+    v.resize(ntiles);
+    info = v.data();
+  }
+  npar[0] = npar[1] = 0;
+  size_t k = 0;
+  for (size_t gi = 0; gi < grids.size(); ++gi) {
+    const GridDev& g = grids[gi];
+    for (int tz = 0; tz < g.tiles_z; ++tz)
+      for (int ty = 0; ty < g.tiles_y; ++ty)
+        for (int tx = 0; tx < g.tiles_x; ++tx) {
+          info[k++] = make_int4((int)gi, tx, ty, tz);
+          ++npar[(tx + ty + tz) & 1];
+        }
+  }
+  ts.nlist[0] = npar[0];
+  ts.nlist[1] = npar[1];
+  if (s) {
+    // the staging buffer is rewritten only after the next host sync on `s`
+    if (desc_bytes) JFC_CUDA(cudaMemcpyAsync(ts.d_desc, ts.h_stage, desc_bytes, cudaMemcpyHostToDevice, s));
+    if (info_bytes) JFC_CUDA(cudaMemcpyAsync(ts.d_info, info, info_bytes, cudaMemcpyHostToDevice, s));
+  } else {
+    if (desc_bytes) JFC_CUDA(cudaMemcpy(ts.d_desc, grids.data(), desc_bytes, cudaMemcpyHostToDevice));
+    if (info_bytes) JFC_CUDA(cudaMemcpy(ts.d_info, info, info_bytes, cudaMemcpyHostToDevice));
+  }
   return JFC_OK;
 }
 
@@ -156,8 +206,8 @@ static int pin_reserve(jfc_ctx* ctx, size_t bytes) {
 // one persistent launch, then read back its outcome (the only host sync of a
 // relabel cycle).  On return (relabel) active[g] holds the active tiles of
 // every grid.
-static int run_bfs(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, bool cut, int& passes,
-                   std::vector<int>* active, int* cut_bad, cudaEvent_t ev_done, int* sweeps_done) {
+int engine_bfs(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, bool cut, int& passes,
+               std::vector<int>* active, int* cut_bad, cudaEvent_t ev_done, int* sweeps_done) {
   cudaStream_t s = ctx->stream;
   JFC_CUDA(cudaMemsetAsync(ts.d_flag_bfs[0], 0, sizeof(int) * (size_t)ts.ntiles, s));
   JFC_CUDA(cudaMemsetAsync(ts.d_flag_bfs[1], 0, sizeof(int) * (size_t)ts.ntiles, s));
@@ -189,6 +239,29 @@ static int run_bfs(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, bool cut, int
   return JFC_OK;
 }
 
+int engine_cut(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, std::vector<GridResult>& res, int& passes) {
+  cudaStream_t s = ctx->stream;
+  res.assign(ts.ngrids, GridResult());
+  int bad = 0;
+  int rc = engine_bfs(ctx, ts, p, true, passes, nullptr, &bad, nullptr, nullptr);
+  if (rc) return rc;
+  JFC_CUDA(launch_grid_sums(ts, s));
+  rc = pin_reserve(ctx, sizeof(long long) * 2 * (size_t)ts.ngrids + 64);
+  if (rc) return rc;
+  long long* hs = (long long*)ctx->h_pin;
+  JFC_CUDA(cudaMemcpyAsync(hs, ts.d_grid_sum, sizeof(long long) * 2 * ts.ngrids, cudaMemcpyDeviceToHost, s));
+  JFC_CUDA(cudaStreamSynchronize(s));
+  for (int g = 0; g < ts.ngrids; ++g) {
+    res[g].neg_sum = hs[2 * g];
+    res[g].labels = hs[2 * g + 1];
+  }
+  if (bad) {
+    rc = set_error(JFC_ERR_NOT_CONVERGED, "cut BFS reached a deficit node");
+    for (auto& r : res) r.status = rc;
+  }
+  return rc;
+}
+
 namespace {
 struct Timer {
   cudaEvent_t a = nullptr, b = nullptr;
@@ -212,7 +285,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
 
   // initial global relabel (exact sink distances; fills the work queues)
   JFC_CUDA(cudaEventRecord(t_gr.a, s));
-  rc = run_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, t_gr.b, nullptr);
+  rc = engine_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, t_gr.b, nullptr);
   if (rc) return rc;
   st.ms_global_relabel += elapsed_ms(t_gr.a, t_gr.b);
   st.global_relabels = 1;
@@ -237,7 +310,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
     // global relabel + active-tile count (one host read-back per cycle)
     JFC_CUDA(cudaEventRecord(t_gr.a, s));
     int sw = 0;
-    rc = run_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, t_gr.b, &sw);
+    rc = engine_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, t_gr.b, &sw);
     if (rc) return rc;
     st.sweeps += sw;
     if (total() * 256 < (long long)ts.ntiles) interval = std::min(interval * 2, p.relabel_interval_max);
@@ -257,7 +330,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   // canonical cut: nodes reachable from excess in the final residual graph
   int bad = 0;
   JFC_CUDA(cudaEventRecord(t_cut.a, s));
-  rc = run_bfs(ctx, ts, p, true, st.bfs_passes, nullptr, &bad, nullptr, nullptr);
+  rc = engine_bfs(ctx, ts, p, true, st.bfs_passes, nullptr, &bad, nullptr, nullptr);
   if (rc) return rc;
   JFC_CUDA(launch_grid_sums(ts, s));
   JFC_CUDA(cudaEventRecord(t_cut.b, s));

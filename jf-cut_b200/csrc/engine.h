@@ -56,8 +56,20 @@ struct GridResult {
 // Solve every grid of `ts` to the exact max-flow (engine.cpp).
 int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, std::vector<GridResult>& res,
                  jfc_stats& st);
-// Build / free a tile set over grids (all of one dimensionality).
-int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDev>& grids);
+// One BFS to its fixpoint in one persistent launch and its read-back: global
+// relabel (cut = false; active[g] = active tiles of grid g afterwards) or the
+// source-side cut (cut = true).  sweeps_done reports the sweeps of the
+// push-relabel phase that ran before it.
+int engine_bfs(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, bool cut, int& passes,
+               std::vector<int>* active, int* cut_bad, cudaEvent_t ev_done, int* sweeps_done);
+// Cut BFS + per-grid sums (min(e, 0), source-side count) of every grid of ts.
+int engine_cut(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, std::vector<GridResult>& res, int& passes);
+// Build / free a tile set over grids (all of one dimensionality).  The control
+// block is reused while it is large enough.  With a stream the grid and tile
+// tables are uploaded asynchronously from pinned staging (rewrite it only
+// after the next host sync on that stream) and a new block gets headroom.
+int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDev>& grids,
+                  cudaStream_t s = nullptr);
 void tileset_free(TileSet& ts);
 int shape_code(int dims, int tile_rows);
 
@@ -70,4 +82,14 @@ int cuda_status(cudaError_t e, const char* where);
   } while (0)
 
 void fill_defaults(jfc_params& p);
+
+// solver.cpp: graph layout, capacity build and plane copies
+size_t align256(size_t v);
+size_t state_bytes(int dims, int w, int h, int d);
+void model_defaults(jfc_model& m);
+int build_core(jfc_graph* G, const void* img, int pixfmt, const uint8_t* seeds, const jfc_model* mdl,
+               cudaMemcpyKind kind);
+// Copy a dense array into (to_dense false) or out of a padded plane of G.
+cudaError_t copy_plane(void* padded, const void* dense, size_t elem, const jfc_graph* G, bool to_dense,
+                       cudaMemcpyKind kind, cudaStream_t s);
 double elapsed_ms(cudaEvent_t a, cudaEvent_t b);

@@ -78,6 +78,9 @@ struct TileSet {
   DevCounters* d_ctr = nullptr;
   void* d_block = nullptr;           // single allocation backing the above
   size_t block_bytes = 0;
+  int cap_tiles = 0, cap_grids = 0;  // capacity of d_block (reused while it fits)
+  void* h_stage = nullptr;           // pinned staging of d_desc / d_info uploads
+  size_t h_stage_bytes = 0;
 };
 
 // Counts every kernel launch of the library (engine.cpp).

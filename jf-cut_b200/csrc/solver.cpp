@@ -16,8 +16,6 @@
 
 #include "engine.h"
 
-namespace {
-
 size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
 void grid_layout(int dims, int w, int h, int d, int& pitch, int& Hp, int& Dp) {
@@ -124,13 +122,15 @@ int build_core(jfc_graph* G, const void* img, int pixfmt, const uint8_t* seeds, 
   JFC_CUDA(cudaMemcpyAsync(M.d_seeds, seeds, n, kind, s));
   M.valid = false;
 
+  // build temporaries are stream-ordered (no device-wide sync on free, so a
+  // build overlaps other streams' kernels)
   BuildScratch* d_bs = nullptr;
-  JFC_CUDA(cudaMalloc((void**)&d_bs, sizeof(BuildScratch)));
+  JFC_CUDA(cudaMallocAsync((void**)&d_bs, sizeof(BuildScratch), s));
   BuildScratch hbs;
   std::memset(&hbs, 0, sizeof(hbs));
   for (int i = 0; i < 12; ++i) hbs.minmax[i] = (i & 1) ? -1 : 0x7fffffff;
   std::vector<void*> temps{d_bs};
-  auto cleanup = [&]() { for (void* p : temps) cudaFree(p); };
+  auto cleanup = [&]() { for (void* p : temps) cudaFreeAsync(p, s); };
   auto fail = [&](int code) { cleanup(); return code; };
 #define JFC_B(call) do { cudaError_t _e = (call); if (_e != cudaSuccess) return fail(cuda_status(_e, #call)); } while (0)
 
@@ -150,11 +150,11 @@ int build_core(jfc_graph* G, const void* img, int pixfmt, const uint8_t* seeds, 
   std::vector<int> lz = G->dims == 3 ? nlink_table(pixfmt, scale_z, sigma2) : std::vector<int>();
   int* d_lxy = nullptr;
   int* d_lz = nullptr;
-  JFC_B(cudaMalloc((void**)&d_lxy, sizeof(int) * lxy.size()));
+  JFC_B(cudaMallocAsync((void**)&d_lxy, sizeof(int) * lxy.size(), s));
   temps.push_back(d_lxy);
   JFC_B(cudaMemcpyAsync(d_lxy, lxy.data(), sizeof(int) * lxy.size(), cudaMemcpyHostToDevice, s));
   if (!lz.empty()) {
-    JFC_B(cudaMalloc((void**)&d_lz, sizeof(int) * lz.size()));
+    JFC_B(cudaMallocAsync((void**)&d_lz, sizeof(int) * lz.size(), s));
     temps.push_back(d_lz);
     JFC_B(cudaMemcpyAsync(d_lz, lz.data(), sizeof(int) * lz.size(), cudaMemcpyHostToDevice, s));
   }
@@ -163,7 +163,7 @@ int build_core(jfc_graph* G, const void* img, int pixfmt, const uint8_t* seeds, 
   const unsigned long long nf = hbs.count[0], nb = hbs.count[1];
   if (nf == 0 || nb == 0) { cleanup(); return set_error(JFC_ERR_NO_SEEDS, "no labels: a seed class is empty"); }
   uint32_t* d_list = nullptr;
-  JFC_B(cudaMalloc((void**)&d_list, sizeof(uint32_t) * (nf + nb)));
+  JFC_B(cudaMallocAsync((void**)&d_list, sizeof(uint32_t) * (nf + nb), s));
   temps.push_back(d_list);
   JFC_B(launch_seed_stats(G->g, M.d_img, pixfmt, M.d_seeds, d_bs->minmax, d_bs->count, d_list, d_list + nf,
                           d_bs->fill, true, s));
@@ -262,8 +262,6 @@ int set_core(jfc_graph* G, const int32_t* e, const int32_t* const* ncap, int64_t
   G->state = 1;
   return JFC_OK;
 }
-
-}  // namespace
 
 extern "C" {
 
@@ -371,7 +369,9 @@ int jfc_graph_create_grid(jfc_ctx* c, int dims, int w, int h, int d, int conn, j
   G->state_bytes = state_bytes(dims, w, h, d);
   cudaError_t e = cudaMalloc(&G->d_state, G->state_bytes);
   if (e != cudaSuccess) { delete G; return cuda_status(e, "graph allocation"); }
-  cudaMemset(G->d_state, 0, G->state_bytes);
+  // zeroed on the context's stream, ordered before every later use of it
+  e = cudaMemsetAsync(G->d_state, 0, G->state_bytes, c->stream);
+  if (e != cudaSuccess) { cudaFree(G->d_state); delete G; return cuda_status(e, "graph clear"); }
   char* p = (char*)G->d_state;
   GridDev& g = G->g;
   std::memset(&g, 0, sizeof(g));
@@ -503,7 +503,7 @@ int jfc_edit_tlinks(jfc_graph* G, const uint32_t* idx, const int32_t* dcs, const
   cudaStream_t s = G->ctx->stream;
   char* buf = nullptr;
   const size_t bytes = align256(n * 4) * 3 + 256;
-  JFC_CUDA(cudaMalloc((void**)&buf, bytes));
+  JFC_CUDA(cudaMallocAsync((void**)&buf, bytes, s));
   uint32_t* d_idx = (uint32_t*)buf;
   int32_t* d_dcs = (int32_t*)(buf + align256(n * 4));
   int32_t* d_dct = (int32_t*)(buf + 2 * align256(n * 4));
@@ -516,7 +516,7 @@ int jfc_edit_tlinks(jfc_graph* G, const uint32_t* idx, const int32_t* dcs, const
   long long ds = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&ds, d_ds, sizeof(ds), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  cudaFree(buf);
+  cudaFreeAsync(buf, s);
   if (e != cudaSuccess) return cuda_status(e, "edit t-links");
   G->sink_total += ds;
   G->state = 1;
@@ -544,7 +544,7 @@ int jfc_graph_edit_seeds(jfc_graph* G, const uint32_t* idx, const uint8_t* new_s
   JFC_CUDA(cudaSetDevice(G->ctx->device));
   cudaStream_t s = G->ctx->stream;
   char* buf = nullptr;
-  JFC_CUDA(cudaMalloc((void**)&buf, align256(m * 4) + align256(m) + 256));
+  JFC_CUDA(cudaMallocAsync((void**)&buf, align256(m * 4) + align256(m) + 256, s));
   uint32_t* d_idx = (uint32_t*)buf;
   uint8_t* d_new = (uint8_t*)(buf + align256(m * 4));
   long long* d_ds = (long long*)(buf + align256(m * 4) + align256(m));
@@ -557,7 +557,7 @@ int jfc_graph_edit_seeds(jfc_graph* G, const uint32_t* idx, const uint8_t* new_s
   long long ds = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&ds, d_ds, sizeof(ds), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  cudaFree(buf);
+  cudaFreeAsync(buf, s);
   if (e != cudaSuccess) return cuda_status(e, "edit seeds");
   G->sink_total += ds;
   G->state = 1;

@@ -59,6 +59,15 @@ class RequestInfo(ctypes.Structure):
                 ("ms_solve", ctypes.c_double), ("ms_total", ctypes.c_double), ("warm", ctypes.c_int)]
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [("budget", ctypes.c_size_t), ("used", ctypes.c_size_t), ("peak_used", ctypes.c_size_t),
+                ("sessions", ctypes.c_int), ("waiting", ctypes.c_int), ("solving", ctypes.c_int),
+                ("peak_solving", ctypes.c_int), ("loops", ctypes.c_int64), ("requests_done", ctypes.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _LIB = None
 VP = ctypes.c_void_p
 I32P = ctypes.POINTER(ctypes.c_int32)
@@ -123,6 +132,7 @@ def _lib():
         L.jfc_server_read_labels.argtypes = [VP, ctypes.c_int, U8P]
         L.jfc_server_close.argtypes = [VP, ctypes.c_int]
         L.jfc_server_cancel.argtypes = [VP, ctypes.c_int]
+        L.jfc_server_get_stats.argtypes = [VP, ctypes.POINTER(ServerStats)]
         L.jfc_synth_gray_ellipse.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int, U8P, U8P]
         L.jfc_synth_rgb_ellipses.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
                                              ctypes.c_int, ctypes.c_int, U8P, U8P]
@@ -404,10 +414,19 @@ class Server:
                "jfc_server_edit")
 
     def wait(self, sid, timeout_ms=-1):
+        """Wait for the session's latest request; returns its RequestInfo (a
+        failed or cancelled request is reported in info.status, not raised)."""
         info = RequestInfo()
+        info.status = -1
         rc = _lib().jfc_server_wait(self.handle, int(sid), int(timeout_ms), ctypes.byref(info))
-        _check(rc, "jfc_server_wait")
+        if rc != OK and info.status != rc:
+            _check(rc, "jfc_server_wait")
         return info
+
+    def stats(self):
+        st = ServerStats()
+        _check(_lib().jfc_server_get_stats(self.handle, ctypes.byref(st)), "jfc_server_get_stats")
+        return st.as_dict()
 
     def labels(self, sid, shape):
         out = np.empty(int(np.prod(shape)), np.uint8)
@@ -430,6 +449,13 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def graph_bytes(shape):
+    """Device bytes of a grid graph's resident state (shape (h, w) or (d, h, w))."""
+    if len(shape) == 2:
+        return int(_lib().jfc_graph_bytes(2, int(shape[1]), int(shape[0]), 1))
+    return int(_lib().jfc_graph_bytes(3, int(shape[2]), int(shape[1]), int(shape[0])))
 
 
 # ---------------------------------------------------------------- synthetic inputs

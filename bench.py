@@ -163,6 +163,215 @@ def cpu_baseline_bk():
                       "workload x%d, init+maxflow+labels" % (shape[1], shape[0], reps)}
 
 
+def pct(v, q):
+    return float(np.percentile(np.asarray(v, dtype=np.float64), q)) if len(v) else None
+
+
+def bench_batched(jfcut, torch, ctx, stream, steps, warmup, n_inst=256):
+    """Batched workload: n_inst independent 2D 4-conn RGB instances with sides
+    drawn uniformly in [128, 2048] (seeded), generated like the plain workload.
+    Batched = every instance in one persistent launch per phase (device work
+    queue, CUDA-graph cycles, autotuned schedule); plain = the same graphs
+    solved one after another with the same schedule.  Both time the solve only
+    (capacity build untimed between steps: it is the same per-instance work in
+    both); every flow and cut of the batch must equal the plain ones."""
+    rng = np.random.default_rng(SEED + 256)
+    sides = rng.integers(128, 2049, size=(n_inst, 2))
+    graphs, dev, total = [], [], 0
+    for i, (w, h) in enumerate(sides):
+        w, h = int(w), int(h)
+        img, seeds = make_workload(w, h, SEED + 5000 + i)
+        dev.append((torch.from_numpy(img).cuda(), torch.from_numpy(seeds).cuda()))
+        graphs.append(jfcut.Graph(ctx, (h, w)))
+        total += w * h
+    offs = np.concatenate([[0], np.cumsum([g.shape[0] * g.shape[1] for g in graphs])])
+    lab_plain = torch.empty(total, dtype=torch.uint8, device="cuda")
+    lab_batch = torch.empty(total, dtype=torch.uint8, device="cuda")
+
+    def build_all():
+        for g, (di, ds) in zip(graphs, dev):
+            g.build_from_device(di.data_ptr(), ds.data_ptr(), jfcut.PIX_RGB8, MODEL)
+        torch.cuda.synchronize()
+
+    def read_all(buf):
+        for i, g in enumerate(graphs):
+            g.read_labels_device(buf[int(offs[i]):].data_ptr())
+
+    build_all()
+    b = jfcut.Batch(ctx)
+    for g in graphs:
+        b.add(g)
+    t0 = time.perf_counter()
+    tuned = b.autotune()
+    t_tune = time.perf_counter() - t0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = jfcut.kernel_launches()
+    ms_plain = []
+    for it in range(warmup + steps):
+        build_all()
+        ev0.record(stream)
+        for g in graphs:
+            g.solve()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if it >= warmup:
+            ms_plain.append(ev0.elapsed_time(ev1))
+    launches_plain = (jfcut.kernel_launches() - l0) / (warmup + steps)
+    flows_plain = [g.flow() for g in graphs]
+    read_all(lab_plain)
+    ms_batch = []
+    l0 = jfcut.kernel_launches()
+    for it in range(warmup + steps):
+        build_all()
+        ev0.record(stream)
+        st = b.solve()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if it >= warmup:
+            ms_batch.append(ev0.elapsed_time(ev1))
+    launches_batch = (jfcut.kernel_launches() - l0) / (warmup + steps)
+    read_all(lab_batch)
+    torch.cuda.synchronize()
+    exact = all(g.flow() == f for g, f in zip(graphs, flows_plain)) and bool(torch.equal(lab_plain, lab_batch))
+    mp, mb = float(np.mean(ms_plain)), float(np.mean(ms_batch))
+    out = {"workload": "%d x 2D 4-conn RGB, sides U[128,2048], seeded; solve only" % n_inst,
+           "instances": n_inst, "nodes": int(total),
+           "plain_ms": mp, "batched_ms": mb,
+           "plain_mnodes_s": total / (mp / 1e3) / 1e6, "batched_mnodes_s": total / (mb / 1e3) / 1e6,
+           "speedup": mp / mb, "bit_exact_vs_plain": exact,
+           "launches_per_step": {"plain": launches_plain, "batched": launches_batch},
+           "used_graph": int(st[0].used_graph), "autotune_s": t_tune,
+           "schedule": {k: getattr(tuned, k) for k in ("tile_rows", "local_iters", "relabel_interval")}}
+    b.close()
+    for g in graphs:
+        g.close()
+    return out
+
+
+def bench_serve(jfcut, torch, ctx, n_req=48, rate=200.0, budget_gb=96):
+    """Serving workload: Poisson arrivals (mean `rate`/s) of n_req sessions,
+    70% 2D RGB images (sides U[256,4096], 4-conn) and 30% int16 phantom
+    volumes (sides U[128,512], 6-conn, N(0,10) noise); each session then sends
+    1-5 stroke edits (0.1-2% of its nodes) one after another, re-solved warm
+    on the device-resident residual graph.  Latency is per request, client
+    side of the C ABI (submit -> result); throughput is all solved nodes over
+    the wall time of the run.  Each session's final flow is checked against a
+    cold plain solve of the same edited graph."""
+    rng = np.random.default_rng(SEED + 200)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    sess = []
+    for i in range(n_req):
+        if rng.random() < 0.7:
+            w, h = (int(v) for v in rng.integers(256, 4097, 2))
+            img, seeds = make_workload(w, h, SEED + 9000 + i)
+            pf = jfcut.PIX_RGB8
+        else:
+            w, h, d = (int(v) for v in rng.integers(128, 513, 3))
+            img, seeds = jfcut.synth_i16_phantom(w, h, d, seed=SEED + 9000 + i, noise_sigma=10)
+            pf = jfcut.PIX_I16
+        n = seeds.size
+        edits = []
+        for k in range(int(rng.integers(1, 6))):
+            m = max(1, int(n * rng.uniform(0.001, 0.02)))
+            edits.append(jfcut.synth_stroke(seeds.shape, seed=SEED + 100 * i + k, n=m, label=1 + (k % 2)))
+        sess.append(dict(img=img, seeds=seeds, pf=pf, edits=edits, n=n, dims=seeds.ndim))
+    srv = jfcut.Server(ctx, int(budget_gb * (1 << 30)), max_slots=64)
+    records = []
+    lock = threading.Lock()
+    t_start = time.perf_counter()
+
+    def client(i):
+        s = sess[i]
+        delay = arrivals[i] - (time.perf_counter() - t_start)
+        if delay > 0:
+            time.sleep(delay)
+        sid = srv.submit(s["img"], s["seeds"], s["pf"], MODEL)
+        info = srv.wait(sid)
+        rec = [("cold", s["n"], s["dims"], info.ms_total, info.status)]
+        for idx, ns in s["edits"]:
+            srv.edit(sid, idx, ns)
+            info = srv.wait(sid)
+            rec.append(("warm", s["n"], s["dims"], info.ms_total, info.status))
+        s["sid"], s["flow"] = sid, info.flow
+        with lock:
+            records.extend(rec)
+
+    threads = [threading.Thread(target=client, args=(i,)) for i in range(n_req)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    wall = time.perf_counter() - t_start
+    sstats = srv.stats()
+    # bit-exactness: every session's final flow equals a cold plain solve of
+    # the same edited graph; labels compared on every 4th session
+    exact = True
+    for j, s in enumerate(sess):
+        g = jfcut.Graph(ctx, s["seeds"].shape)
+        g.build_from_image(s["img"], s["seeds"], s["pf"], MODEL)
+        for idx, ns in s["edits"]:
+            g.edit_seeds(idx, ns)
+        g.solve()
+        exact &= g.flow() == s["flow"]
+        if j % 4 == 0:
+            exact &= bool(np.array_equal(g.labels(), srv.labels(s["sid"], s["seeds"].shape)))
+        g.close()
+        srv.close_session(s["sid"])
+    srv.close()
+    ok = all(r[4] == 0 for r in records)
+    cold = [r[3] for r in records if r[0] == "cold"]
+    warm = [r[3] for r in records if r[0] == "warm"]
+    nodes = sum(r[1] for r in records)
+    return {"workload": "Poisson %.0f req/s, %d sessions (70%% 2D RGB 256-4096 sides, 30%% int16 volumes "
+                        "128-512 sides), 1-5 warm stroke edits each (0.1-2%% of nodes)" % (rate, n_req),
+            "requests": len(records), "all_ok": ok, "bit_exact_vs_cold_plain": bool(exact),
+            "cold_p50_ms": pct(cold, 50), "cold_p99_ms": pct(cold, 99),
+            "warm_p50_ms": pct(warm, 50), "warm_p99_ms": pct(warm, 99),
+            "throughput_mnodes_s": nodes / wall / 1e6, "wall_s": wall,
+            "budget_gb": budget_gb, "peak_used_gb": sstats["peak_used"] / 2**30,
+            "peak_solving": sstats["peak_solving"], "loops": sstats["loops"]}
+
+
+def bench_edit4096(jfcut, torch, ctx, n_edits=30):
+    """Interactive edits at 4096^2: one 2D RGB session, n_edits sequential
+    stroke edits (0.1-2% of nodes each) re-solved warm in the server, against
+    a cold plain re-solve (build + the same edits + solve) of the same graph;
+    flows must agree."""
+    w = h = 4096
+    img, seeds = make_workload(w, h, SEED + 4096)
+    rng = np.random.default_rng(SEED + 4097)
+    edits = []
+    for k in range(n_edits):
+        m = max(1, int(w * h * rng.uniform(0.001, 0.02)))
+        edits.append(jfcut.synth_stroke(seeds.shape, seed=SEED + 7000 + k, n=m, label=1 + (k % 2)))
+    srv = jfcut.Server(ctx, 0, max_slots=8)
+    sid = srv.submit(img, seeds, jfcut.PIX_RGB8, MODEL)
+    cold_first = srv.wait(sid).ms_total
+    warm, flows = [], []
+    for idx, ns in edits:
+        srv.edit(sid, idx, ns)
+        info = srv.wait(sid)
+        warm.append(info.ms_total)
+        flows.append(info.flow)
+    srv.close()
+    cold, exact = [], True
+    for k in range(4, n_edits, max(1, n_edits // 5)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g = jfcut.Graph(ctx, (h, w))
+        g.build_from_image(img, seeds, jfcut.PIX_RGB8, MODEL)
+        for idx, ns in edits[:k + 1]:
+            g.edit_seeds(idx, ns)
+        g.solve()
+        cold.append((time.perf_counter() - t0) * 1e3)
+        exact &= g.flow() == flows[k]
+        g.close()
+    return {"workload": "2D 4-conn RGB 4096x4096, %d sequential stroke edits (0.1-2%% of nodes)" % n_edits,
+            "first_solve_ms": cold_first, "warm_p50_ms": pct(warm, 50), "warm_p99_ms": pct(warm, 99),
+            "cold_resolve_p50_ms": pct(cold, 50), "cold_resolve_p99_ms": pct(cold, 99),
+            "cold_samples": len(cold), "bit_exact_vs_cold": bool(exact)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -172,6 +381,9 @@ def main():
     ap.add_argument("--width", type=int, default=W_FULL)
     ap.add_argument("--height", type=int, default=H_FULL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--extras", default="batched,serve,edit4096",
+                    help="comma list of extra sections at N=1 (batched, serve, edit4096) or 'none'")
+    ap.add_argument("--serve-requests", type=int, default=48)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -301,6 +513,19 @@ def main():
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_bk()
+        extras = [] if world > 1 or args.extras == "none" else args.extras.split(",")
+        sections = {"batched": lambda: bench_batched(jfcut, torch, ctx, stream, 2, 1),
+                    "edit4096": lambda: bench_edit4096(jfcut, torch, ctx),
+                    "serve": lambda: bench_serve(jfcut, torch, ctx, n_req=args.serve_requests)}
+        with torch.cuda.stream(stream):
+            for name in ("batched", "edit4096", "serve"):
+                if name in extras:
+                    t0 = time.perf_counter()
+                    try:
+                        line[name] = sections[name]()
+                    except Exception as ex:   # a failed section is reported, the headline stands
+                        line[name] = {"error": "%s: %s" % (type(ex).__name__, ex)}
+                    line[name]["section_s"] = time.perf_counter() - t0
         print(json.dumps(line), flush=True)
     g.close()
     ctx.close()

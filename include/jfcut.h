@@ -76,7 +76,8 @@ typedef struct jfc_params {
   int relabel_interval;  /* sweep pairs between global relabels at the start (default 4) */
   int max_sweeps;        /* budget of sweeps -> JFC_ERR_NOT_CONVERGED (default 1<<20) */
   int max_bfs_passes;    /* budget of tile passes per BFS (default 1<<20) */
-  int use_graph;         /* reserved (0) */
+  int use_graph;         /* 1: replay each relabel cycle (push-relabel phase + global
+                            relabel + read-back) as one CUDA graph launch (default) */
   int verbose;           /* 1: one JSON line per global relabel on stderr */
   int relabel_interval_max; /* adaptive interval cap: the interval doubles while fewer
                                than 1/256 of the tiles are active (default 16 x interval) */
@@ -111,6 +112,7 @@ typedef struct jfc_stats {
   long long bfs_visits;   /* tile visits of all BFS passes */
   double ms_gr_first;     /* global relabel: dense first passes (device clock) */
   double ms_gr_frontier;  /* global relabel: frontier passes (device clock) */
+  int used_graph;         /* 1 if the relabel cycles ran as CUDA graph launches */
 } jfc_stats;
 
 typedef struct jfc_ctx jfc_ctx;

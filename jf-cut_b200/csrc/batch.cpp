@@ -155,26 +155,48 @@ int jfc_batch_autotune(jfc_batch* b, jfc_params* chosen) {
   int rc = snapshot(b, snap, false);
   if (rc) return rc;
   const jfc_params base = b->ctx->params;
+  // one timed solve of the batch from the snapshot under schedule p
+  auto trial = [&](const jfc_params& p, double& ms) -> int {
+    b->ctx->params = p;
+    b->ctx->params.relabel_interval_max = 0;   // re-derived from the trial interval
+    fill_defaults(b->ctx->params);
+    int r = snapshot(b, snap, true);
+    if (r) return r;
+    const auto t0 = std::chrono::steady_clock::now();
+    r = jfc_batch_solve(b, nullptr);
+    const auto t1 = std::chrono::steady_clock::now();
+    ms = r ? 1e30 : std::chrono::duration<double, std::milli>(t1 - t0).count();
+    return r == JFC_ERR_NOT_CONVERGED ? JFC_OK : r;
+  };
+  // Coordinate descent from the context's schedule: relabel interval, then
+  // rounds per visit, then tile height; each axis keeps its best value.  The
+  // first trial also pays one-time costs (tile set, graph capture), so the
+  // starting point is timed twice.
   jfc_params best = base;
-  double best_ms = 1e30;
-  const int rows[] = {8, 16};
-  const int iters[] = {8, 16, 32};
+  double best_ms = 1e30, ms = 0.0;
+  rc = trial(best, ms);
+  if (rc) { b->ctx->params = base; return rc; }
+  rc = trial(best, best_ms);
+  if (rc) { b->ctx->params = base; return rc; }
   const int intervals[] = {2, 4, 8, 16};
-  for (int tr : rows)
-    for (int li : iters)
-      for (int ri : intervals) {
-        jfc_params p = base;
-        p.tile_rows = tr; p.local_iters = li; p.relabel_interval = ri;
-        b->ctx->params = p;
-        rc = snapshot(b, snap, true);
-        if (rc) { b->ctx->params = base; return rc; }
-        auto t0 = std::chrono::steady_clock::now();
-        rc = jfc_batch_solve(b, nullptr);
-        auto t1 = std::chrono::steady_clock::now();
-        if (rc) continue;
-        const double ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-        if (ms < best_ms) { best_ms = ms; best = p; }
-      }
+  const int iters[] = {8, 16, 32};
+  const int rows[] = {8, 16};
+  for (int axis = 0; axis < 3; ++axis) {
+    const int* vals = axis == 0 ? intervals : axis == 1 ? iters : rows;
+    const int nv = axis == 0 ? 4 : axis == 1 ? 3 : 2;
+    const jfc_params center = best;
+    for (int i = 0; i < nv; ++i) {
+      jfc_params p = center;
+      int& field = axis == 0 ? p.relabel_interval : axis == 1 ? p.local_iters : p.tile_rows;
+      if (field == vals[i]) continue;
+      field = vals[i];
+      rc = trial(p, ms);
+      if (rc) { b->ctx->params = base; return rc; }
+      if (ms < best_ms) { best_ms = ms; best = p; }
+    }
+  }
+  best.relabel_interval_max = 0;
+  fill_defaults(best);
   b->ctx->params = best;
   rc = snapshot(b, snap, true);
   for (jfc_graph* g : b->graphs) g->state = 1;

@@ -29,7 +29,13 @@
 static thread_local std::string g_err;
 static std::atomic<unsigned long long> g_launches{0};
 
-void jfc_note_launch(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+// launches recorded while a stream is captured run later as graph nodes and
+// are counted when the graph is launched
+static thread_local bool g_capturing = false;
+
+void jfc_note_launch(int n) {
+  if (!g_capturing) g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed);
+}
 
 extern "C" unsigned long long jfc_kernel_launches(void) { return g_launches.load(); }
 
@@ -67,6 +73,7 @@ int shape_code(int dims, int tile_rows) { return dims * 100 + tile_rows; }
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 void tileset_free(TileSet& ts) {
+  tileset_drop_graphs(ts);
   if (ts.d_block) cudaFree(ts.d_block);
   if (ts.h_stage) cudaFreeHost(ts.h_stage);
   ts = TileSet();
@@ -145,6 +152,7 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDe
     tileset_carve(ts, blk, &total);
     JFC_CUDA(cudaMemset(blk, 0, total));
   }
+  tileset_drop_graphs(ts);   // captured launches hold the old tile set by value
   ts.dims = dims;
   ts.TR = tile_rows; ts.TY = TY; ts.TZ = TZ;
   ts.ngrids = ngrids;
@@ -202,31 +210,37 @@ static int pin_reserve(jfc_ctx* ctx, size_t bytes) {
   return JFC_OK;
 }
 
-// Run one BFS (global relabel when !cut, cut otherwise) to its fixpoint in
-// one persistent launch, then read back its outcome (the only host sync of a
-// relabel cycle).  On return (relabel) active[g] holds the active tiles of
-// every grid.
-int engine_bfs(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, bool cut, int& passes,
-               std::vector<int>* active, int* cut_bad, cudaEvent_t ev_done, int* sweeps_done) {
-  cudaStream_t s = ctx->stream;
-  JFC_CUDA(cudaMemsetAsync(ts.d_flag_bfs[0], 0, sizeof(int) * (size_t)ts.ntiles, s));
-  JFC_CUDA(cudaMemsetAsync(ts.d_flag_bfs[1], 0, sizeof(int) * (size_t)ts.ntiles, s));
-  if (!cut) JFC_CUDA(cudaMemsetAsync(ts.d_grid_active, 0, sizeof(int) * ts.ngrids, s));
+static size_t pin_need(const TileSet& ts) {
+  return sizeof(DevCounters) + sizeof(long long) * 2 * (size_t)ts.ngrids + 64;
+}
+
+// Enqueue one BFS (global relabel when !cut, cut otherwise) and the read-back
+// of its counters (+ per-grid active tiles) into pinned memory `pin`.
+static cudaError_t enqueue_bfs(TileSet& ts, bool cut, int max_passes, cudaStream_t s, void* pin) {
+  cudaError_t e;
+#define JFC_E(call) do { e = (call); if (e != cudaSuccess) return e; } while (0)
+  JFC_E(cudaMemsetAsync(ts.d_flag_bfs[0], 0, sizeof(int) * (size_t)ts.ntiles, s));
+  JFC_E(cudaMemsetAsync(ts.d_flag_bfs[1], 0, sizeof(int) * (size_t)ts.ntiles, s));
+  if (!cut) JFC_E(cudaMemsetAsync(ts.d_grid_active, 0, sizeof(int) * ts.ngrids, s));
   // reset the BFS part of the control block: tickets, frontiers, status, cut flag
-  JFC_CUDA(cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s));
-  JFC_CUDA(cudaMemsetAsync(ts.d_ctr->qn_bfs, 0, sizeof(ts.d_ctr->qn_bfs), s));
-  JFC_CUDA(cudaMemsetAsync(&ts.d_ctr->bfs_status, 0, sizeof(int), s));
-  if (cut) JFC_CUDA(cudaMemsetAsync(&ts.d_ctr->cut_bad, 0, sizeof(int), s));
-  JFC_CUDA(launch_bfs(ts, cut, p.max_bfs_passes, s));
-  if (ev_done) JFC_CUDA(cudaEventRecord(ev_done, s));
-  const size_t need = sizeof(DevCounters) + sizeof(int) * (size_t)ts.ngrids + 64;
-  int rc = pin_reserve(ctx, need);
-  if (rc) return rc;
-  DevCounters* hc = (DevCounters*)ctx->h_pin;
-  int* hact = (int*)((char*)ctx->h_pin + sizeof(DevCounters));
-  JFC_CUDA(cudaMemcpyAsync(hc, ts.d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
-  if (!cut) JFC_CUDA(cudaMemcpyAsync(hact, ts.d_grid_active, sizeof(int) * ts.ngrids, cudaMemcpyDeviceToHost, s));
-  JFC_CUDA(cudaStreamSynchronize(s));
+  JFC_E(cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s));
+  JFC_E(cudaMemsetAsync(ts.d_ctr->qn_bfs, 0, sizeof(ts.d_ctr->qn_bfs), s));
+  JFC_E(cudaMemsetAsync(&ts.d_ctr->bfs_status, 0, sizeof(int), s));
+  if (cut) JFC_E(cudaMemsetAsync(&ts.d_ctr->cut_bad, 0, sizeof(int), s));
+  JFC_E(launch_bfs(ts, cut, max_passes, s));
+  JFC_E(cudaMemcpyAsync(pin, ts.d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, s));
+  if (!cut)
+    JFC_E(cudaMemcpyAsync((char*)pin + sizeof(DevCounters), ts.d_grid_active, sizeof(int) * ts.ngrids,
+                          cudaMemcpyDeviceToHost, s));
+#undef JFC_E
+  return cudaSuccess;
+}
+
+// Outcome of a BFS from the pinned read-back (after the stream sync).
+static int finish_bfs(const TileSet& ts, bool cut, const void* pin, int& passes, std::vector<int>* active,
+                      int* cut_bad, int* sweeps_done) {
+  const DevCounters* hc = (const DevCounters*)pin;
+  const int* hact = (const int*)((const char*)pin + sizeof(DevCounters));
   passes += hc->bfs_passes;
   if (sweeps_done) *sweeps_done = hc->sweeps_done;
   if (hc->error) return set_error(JFC_ERR_CUDA, "grid barrier timed out in a persistent kernel");
@@ -239,14 +253,118 @@ int engine_bfs(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, bool cut, int& pa
   return JFC_OK;
 }
 
+// Run one BFS to its fixpoint in one persistent launch, then read back its
+// outcome (the only host sync of a relabel cycle).  On return (relabel)
+// active[g] holds the active tiles of every grid.
+int engine_bfs(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, bool cut, int& passes,
+               std::vector<int>* active, int* cut_bad, int* sweeps_done) {
+  cudaStream_t s = ctx->stream;
+  int rc = pin_reserve(ctx, pin_need(ts));
+  if (rc) return rc;
+  JFC_CUDA(enqueue_bfs(ts, cut, p.max_bfs_passes, s, ctx->h_pin));
+  JFC_CUDA(cudaStreamSynchronize(s));
+  return finish_bfs(ts, cut, ctx->h_pin, passes, active, cut_bad, sweeps_done);
+}
+
+// ---- CUDA graphs of the relabel cycle -------------------------------------
+// One cycle = { push-relabel phase (interval sweeps), global relabel, counter
+// read-back }: ~10 stream operations between two host syncs.  They are
+// captured once per (interval, local_iters, pass budget, read-back buffer)
+// and replayed with one graph launch.  The cache belongs to the tile set and
+// is dropped whenever the tile set changes.
+namespace {
+struct CycleGraphs {
+  struct Entry {
+    int interval, local_iters, max_passes;
+    void* pin;
+    cudaGraphExec_t exec;
+  };
+  std::vector<Entry> v;
+  bool broken = false;   // capture not available on this stream: direct launches
+};
+}  // namespace
+
+void tileset_drop_graphs(TileSet& ts) {
+  if (!ts.gcache) return;
+  CycleGraphs* c = (CycleGraphs*)ts.gcache;
+  for (auto& e : c->v) cudaGraphExecDestroy(e.exec);
+  delete c;
+  ts.gcache = nullptr;
+}
+
+static cudaError_t enqueue_cycle(TileSet& ts, int interval, int local_iters, int max_passes, cudaStream_t s,
+                                 void* pin) {
+  cudaError_t e = cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s);
+  if (e == cudaSuccess) e = launch_pr_phase(ts, interval, local_iters, s);
+  if (e == cudaSuccess) e = enqueue_bfs(ts, false, max_passes, s, pin);
+  return e;
+}
+
+static cudaGraphExec_t cycle_graph(TileSet& ts, int interval, int local_iters, int max_passes, cudaStream_t s,
+                                   void* pin) {
+  if (!ts.gcache) ts.gcache = new CycleGraphs();
+  CycleGraphs* c = (CycleGraphs*)ts.gcache;
+  if (c->broken) return nullptr;
+  for (auto& e : c->v)
+    if (e.interval == interval && e.local_iters == local_iters && e.max_passes == max_passes && e.pin == pin)
+      return e.exec;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    c->broken = true;   // the caller is capturing this stream itself
+    return nullptr;
+  }
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    c->broken = true;
+    return nullptr;
+  }
+  g_capturing = true;
+  const cudaError_t e1 = enqueue_cycle(ts, interval, local_iters, max_passes, s, pin);
+  g_capturing = false;
+  cudaGraph_t g = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(s, &g);
+  cudaGraphExec_t x = nullptr;
+  if (e1 == cudaSuccess && e2 == cudaSuccess && g) {
+    if (cudaGraphInstantiate(&x, g, 0) != cudaSuccess) x = nullptr;
+  }
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();   // a refused capture leaves no sticky error
+  if (!x) {
+    c->broken = true;
+    return nullptr;
+  }
+  c->v.push_back({interval, local_iters, max_passes, pin, x});
+  return x;
+}
+
+// One relabel cycle, replayed from a graph when enabled; returns the outcome
+// of its global relabel.
+static int run_cycle(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, int interval, int& passes,
+                     std::vector<int>& active, int* sweeps_done, bool* used_graph) {
+  cudaStream_t s = ctx->stream;
+  int rc = pin_reserve(ctx, pin_need(ts));
+  if (rc) return rc;
+  cudaGraphExec_t x = p.use_graph ? cycle_graph(ts, interval, p.local_iters, p.max_bfs_passes, s, ctx->h_pin)
+                                  : nullptr;
+  if (x) {
+    JFC_CUDA(cudaGraphLaunch(x, s));
+    jfc_note_launch(2);
+    if (used_graph) *used_graph = true;
+  } else {
+    JFC_CUDA(enqueue_cycle(ts, interval, p.local_iters, p.max_bfs_passes, s, ctx->h_pin));
+  }
+  JFC_CUDA(cudaStreamSynchronize(s));
+  return finish_bfs(ts, false, ctx->h_pin, passes, &active, nullptr, sweeps_done);
+}
+
 int engine_cut(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, std::vector<GridResult>& res, int& passes) {
   cudaStream_t s = ctx->stream;
   res.assign(ts.ngrids, GridResult());
   int bad = 0;
-  int rc = engine_bfs(ctx, ts, p, true, passes, nullptr, &bad, nullptr, nullptr);
+  int rc = engine_bfs(ctx, ts, p, true, passes, nullptr, &bad, nullptr);
   if (rc) return rc;
   JFC_CUDA(launch_grid_sums(ts, s));
-  rc = pin_reserve(ctx, sizeof(long long) * 2 * (size_t)ts.ngrids + 64);
+  rc = pin_reserve(ctx, pin_need(ts));
   if (rc) return rc;
   long long* hs = (long long*)ctx->h_pin;
   JFC_CUDA(cudaMemcpyAsync(hs, ts.d_grid_sum, sizeof(long long) * 2 * ts.ngrids, cudaMemcpyDeviceToHost, s));
@@ -262,14 +380,6 @@ int engine_cut(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, std::vector<GridR
   return rc;
 }
 
-namespace {
-struct Timer {
-  cudaEvent_t a = nullptr, b = nullptr;
-  Timer() { cudaEventCreate(&a); cudaEventCreate(&b); }
-  ~Timer() { cudaEventDestroy(a); cudaEventDestroy(b); }
-};
-}  // namespace
-
 int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<GridResult>& res,
                  jfc_stats& st) {
   jfc_params p = p_in;
@@ -277,50 +387,54 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   cudaStream_t s = ctx->stream;
   std::memset(&st, 0, sizeof(st));
   res.assign(ts.ngrids, GridResult());
-  Timer t_all, t_pr, t_gr, t_cut;
-  JFC_CUDA(cudaEventRecord(t_all.a, s));
+  cudaEvent_t ev[4];
+  for (auto& e : ev) cudaEventCreate(&e);
+  struct EvFree {
+    cudaEvent_t* e;
+    ~EvFree() { for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]); }
+  } ev_free{ev};
+  JFC_CUDA(cudaEventRecord(ev[0], s));
   JFC_CUDA(launch_clear_counters(ts, s));
   std::vector<int> active;
   int rc;
 
   // initial global relabel (exact sink distances; fills the work queues)
-  JFC_CUDA(cudaEventRecord(t_gr.a, s));
-  rc = engine_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, t_gr.b, nullptr);
+  rc = engine_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, nullptr);
   if (rc) return rc;
-  st.ms_global_relabel += elapsed_ms(t_gr.a, t_gr.b);
   st.global_relabels = 1;
 
   auto total = [&]() { long long t = 0; for (int v : active) t += v; return t; };
+  const DevCounters* hc = (const DevCounters*)ctx->h_pin;
+  double prev_pr = 0.0, prev_gr = 0.0;
   int status = JFC_OK;
   // Adaptive schedule: while a large part of the grid is active, frequent
   // global relabels pay off; once only a sliver is active (long transport
   // paths, few tiles), the dense relabel dominates, so the interval doubles
   // (the push-relabel phase still stops as soon as its queues drain).
   int interval = p.relabel_interval;
+  bool graphs = false;
   while (total() > 0) {
     if (st.sweeps >= p.max_sweeps) {
       status = set_error(JFC_ERR_NOT_CONVERGED, "sweep budget exhausted");
       break;
     }
-    // relabel_interval x (even sweep, odd sweep) in one persistent launch
-    JFC_CUDA(cudaEventRecord(t_pr.a, s));
-    JFC_CUDA(cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s));
-    JFC_CUDA(launch_pr_phase(ts, interval, p.local_iters, s));
-    JFC_CUDA(cudaEventRecord(t_pr.b, s));
-    // global relabel + active-tile count (one host read-back per cycle)
-    JFC_CUDA(cudaEventRecord(t_gr.a, s));
+    // relabel_interval x (even sweep, odd sweep), global relabel, active-tile
+    // count: one host read-back per cycle
     int sw = 0;
-    rc = engine_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, t_gr.b, &sw);
+    rc = run_cycle(ctx, ts, p, interval, st.bfs_passes, active, &sw, &graphs);
     if (rc) return rc;
     st.sweeps += sw;
     if (total() * 256 < (long long)ts.ntiles) interval = std::min(interval * 2, p.relabel_interval_max);
     else interval = p.relabel_interval;
-    st.ms_push_relabel += elapsed_ms(t_pr.a, t_pr.b);
-    st.ms_global_relabel += elapsed_ms(t_gr.a, t_gr.b);
     ++st.global_relabels;
-    if (p.verbose)
+    if (p.verbose) {
+      hc = (const DevCounters*)ctx->h_pin;
+      const double pr = hc->ns_pr * 1e-6, gr = (hc->ns_gr_first + hc->ns_gr_frontier) * 1e-6;
       fprintf(stderr, "{\"relabel\": %d, \"sweeps\": %d, \"active_tiles\": %lld, \"ms_pr\": %.3f, \"ms_gr\": %.3f}\n",
-              st.global_relabels, st.sweeps, total(), elapsed_ms(t_pr.a, t_pr.b), elapsed_ms(t_gr.a, t_gr.b));
+              st.global_relabels, st.sweeps, total(), pr - prev_pr, gr - prev_gr);
+      prev_pr = pr;
+      prev_gr = gr;
+    }
   }
   if (status != JFC_OK) {
     for (int g = 0; g < ts.ngrids; ++g)
@@ -328,35 +442,34 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   }
 
   // canonical cut: nodes reachable from excess in the final residual graph
-  int bad = 0;
-  JFC_CUDA(cudaEventRecord(t_cut.a, s));
-  rc = engine_bfs(ctx, ts, p, true, st.bfs_passes, nullptr, &bad, nullptr, nullptr);
-  if (rc) return rc;
-  JFC_CUDA(launch_grid_sums(ts, s));
-  JFC_CUDA(cudaEventRecord(t_cut.b, s));
-  rc = pin_reserve(ctx, sizeof(long long) * 2 * (size_t)ts.ngrids + 128);
-  if (rc) return rc;
-  long long* hs = (long long*)ctx->h_pin;
-  unsigned long long* hv = (unsigned long long*)(hs + 2 * ts.ngrids);
-  JFC_CUDA(cudaMemcpyAsync(hs, ts.d_grid_sum, sizeof(long long) * 2 * ts.ngrids, cudaMemcpyDeviceToHost, s));
-  JFC_CUDA(cudaMemcpyAsync(hv, &ts.d_ctr->visits, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-  JFC_CUDA(cudaEventRecord(t_all.b, s));
+  JFC_CUDA(cudaEventRecord(ev[2], s));
+  int passes = st.bfs_passes;
+  std::vector<GridResult> cut;
+  rc = engine_cut(ctx, ts, p, cut, passes);
+  if (rc && rc != JFC_ERR_NOT_CONVERGED) return rc;
+  st.bfs_passes = passes;
+  JFC_CUDA(cudaEventRecord(ev[3], s));
+  // device-clock phase times and visit counters
+  unsigned long long* hv = (unsigned long long*)ctx->h_pin;
+  JFC_CUDA(cudaMemcpyAsync(hv, &ts.d_ctr->visits, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  JFC_CUDA(cudaEventRecord(ev[1], s));
   JFC_CUDA(cudaStreamSynchronize(s));
-  st.ms_cut = elapsed_ms(t_cut.a, t_cut.b);
-  st.ms_total = elapsed_ms(t_all.a, t_all.b);
+  st.ms_cut = elapsed_ms(ev[2], ev[3]);
+  st.ms_total = elapsed_ms(ev[0], ev[1]);
   st.tile_visits = (long long)hv[0];
   st.bfs_visits = (long long)hv[1];
   st.pr_rounds = (long long)hv[2];
   st.ms_gr_first = hv[3] * 1e-6;
   st.ms_gr_frontier = hv[4] * 1e-6;
+  st.ms_global_relabel = st.ms_gr_first + st.ms_gr_frontier;
+  st.ms_push_relabel = hv[5] * 1e-6;
+  st.used_graph = graphs ? 1 : 0;
   for (int g = 0; g < ts.ngrids; ++g) {
-    res[g].neg_sum = hs[2 * g];
-    res[g].labels = hs[2 * g + 1];
+    res[g].neg_sum = cut[g].neg_sum;
+    res[g].labels = cut[g].labels;
+    if (cut[g].status && !res[g].status) res[g].status = cut[g].status;
   }
-  if (bad && status == JFC_OK) {
-    status = set_error(JFC_ERR_NOT_CONVERGED, "cut BFS reached a deficit node");
-    for (auto& r : res) r.status = status;
-  }
+  if (rc == JFC_ERR_NOT_CONVERGED && status == JFC_OK) status = rc;
   st.status = status;
   return status;
 }

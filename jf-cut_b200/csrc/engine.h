@@ -61,7 +61,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, std::vector<Gri
 // source-side cut (cut = true).  sweeps_done reports the sweeps of the
 // push-relabel phase that ran before it.
 int engine_bfs(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, bool cut, int& passes,
-               std::vector<int>* active, int* cut_bad, cudaEvent_t ev_done, int* sweeps_done);
+               std::vector<int>* active, int* cut_bad, int* sweeps_done);
 // Cut BFS + per-grid sums (min(e, 0), source-side count) of every grid of ts.
 int engine_cut(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, std::vector<GridResult>& res, int& passes);
 // Build / free a tile set over grids (all of one dimensionality).  The control
@@ -71,6 +71,8 @@ int engine_cut(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, std::vector<GridR
 int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDev>& grids,
                   cudaStream_t s = nullptr);
 void tileset_free(TileSet& ts);
+// Drop the tile set's captured relabel-cycle graphs.
+void tileset_drop_graphs(TileSet& ts);
 int shape_code(int dims, int tile_rows);
 
 int set_error(int code, const std::string& msg);

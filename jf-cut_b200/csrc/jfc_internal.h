@@ -56,6 +56,8 @@ struct DevCounters {
   unsigned long long rounds; // push/relabel rounds summed over visits
   unsigned long long ns_gr_first;     // global relabel: first (dense) pass, device ns
   unsigned long long ns_gr_frontier;  // global relabel: frontier passes + queue refill
+  unsigned long long ns_pr;           // push-relabel phases, device ns
+  unsigned long long t_gr_start;      // device clock at the start of the last relabel
 };
 
 // A set of grids tiled with one tile shape: the unit every launch works on
@@ -81,6 +83,7 @@ struct TileSet {
   int cap_tiles = 0, cap_grids = 0;  // capacity of d_block (reused while it fits)
   void* h_stage = nullptr;           // pinned staging of d_desc / d_info uploads
   size_t h_stage_bytes = 0;
+  void* gcache = nullptr;            // captured relabel-cycle graphs (engine.cpp)
 };
 
 // Counts every kernel launch of the library (engine.cpp).

@@ -344,16 +344,10 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
   const long long tbase = (long long)x0 + (long long)y0 * pitch + (long long)z0 * slab;
   const long long n = tbase + x + (long long)y * pitch + (long long)z * slab;
   const int hi = T::hidx(x, y, z);
-  const int e = g.e[n];
-  unsigned arcs = 0;
-  arcs |= g.r[D::XP][n] > 0 ? jfc::A_XP : 0u;
-  arcs |= g.r[D::YP][n] > 0 ? jfc::A_YP : 0u;
-  arcs |= g.r[D::YM][n] > 0 ? jfc::A_YM : 0u;
-  arcs |= g.r[D::XM][n] > 0 ? jfc::A_XM : 0u;
-  if constexpr (DIMS == 3) {
-    arcs |= g.r[D::ZP][n] > 0 ? jfc::A_ZP : 0u;
-    arcs |= g.r[D::ZM][n] > 0 ? jfc::A_ZM : 0u;
-  }
+  // residual-arc bits and the excess sign, written by the first pass
+  const unsigned ab = g.label[n];
+  const unsigned arcs = ab & 63u;
+  const bool pos = (ab & 128u) != 0;
   s.arc[t] = (uint8_t)arcs;
   const int hstart = g.h[n];
   s.h[hi] = hstart;
@@ -380,7 +374,7 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
     if (DIMS == 3 && z == 0) s.face[4] = 1;
     if (DIMS == 3 && z == TZ - 1) s.face[5] = 1;
   }
-  const bool act = __syncthreads_or((e > 0) & (hf < JFC_INF));
+  const bool act = __syncthreads_or(pos & (hf < JFC_INF));
   if (t < 32) {
     const int txs = g.tiles_x, tys = g.tiles_y;
     bool want = false;
@@ -482,6 +476,17 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
       S1[i] |= (((sb >> (16 + i)) & 1u) << 31) & AXP[i];
     }
   }
+  // the frontier passes read one byte per node instead of e and the residual
+  // planes: bits 0-5 residual arcs (jfc::A_*), bit 7 e > 0 (the label plane
+  // is free until the cut BFS writes it)
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    unsigned b = ((AXP[i] >> lane) & 1u) * jfc::A_XP | ((AYP[i] >> lane) & 1u) * jfc::A_YP |
+                 ((AYM[i] >> lane) & 1u) * jfc::A_YM | ((AXM[i] >> lane) & 1u) * jfc::A_XM |
+                 ((POS[i] >> lane) & 1u) * 128u;
+    if constexpr (DIMS == 3) b |= ((AZP[i] >> lane) & 1u) * jfc::A_ZP | ((AZM[i] >> lane) & 1u) * jfc::A_ZM;
+    g.label[roff<TY>(a, i)] = (uint8_t)b;
+  }
   int h[R];
 #pragma unroll
   for (int i = 0; i < R; ++i) h[i] = ((DEF[i] >> lane) & 1u) ? 0 : JFC_INF;
@@ -534,12 +539,27 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
   flag_neighbours<DIMS, TY, TZ>(g, a, tid, rows_fin, c0 != 0, c31 != 0, false, Q);
 }
 
-// Persistent global relabel: pass 0 initialises and closes every tile (one
-// warp per tile, chunks of 8 tiles per ticket), later passes drain the
-// frontier (one CTA per tile), then the push-relabel queues are refilled with
-// every tile holding an active node (the reference's graphcut_count_node +
-// clogs scan + graphcut_scatter_node, graphcut_count_block.cl:19-65, as one
-// warp-aggregated append).
+// Global relabel, pass 0: every tile, one warp per tile (bit-parallel level
+// BFS from the deficits, fused initialisation).  A plain launch: its many
+// registers do not limit the occupancy of the frontier kernel.
+template <int DIMS, int TY, int TZ>
+__global__ void __launch_bounds__(256, 2) k_relabel_first(TileSet ts) {
+  DevCounters* ctr = ts.d_ctr;
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctr->t_gr_start = jfc::global_ns();
+  const int lane = threadIdx.x & 31;
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= ts.ntiles) return;
+  BfsQ Q{ts.d_flag_bfs[1], ts.d_q_bfs[1], &ctr->qn_bfs[1]};
+  int wgrid = -1, wdelta = 0;
+  relabel_first_warp<DIMS, TY, TZ>(ts, (int)w, Q, wgrid, wdelta);
+  if (lane == 0 && wdelta && wgrid >= 0) atomicAdd(&ts.d_grid_active[wgrid], wdelta);
+}
+
+// Global relabel, frontier passes (persistent, cooperative): one CTA per
+// queued tile, grid barrier between passes, until a pass queues nothing; then
+// the push-relabel queues are refilled with every tile holding an active node
+// (the reference's graphcut_count_node + clogs scan + graphcut_scatter_node,
+// graphcut_count_block.cl:19-65, as one warp-aggregated append).
 template <int DIMS, int TY, int TZ>
 __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts, int max_passes) {
   __shared__ RlSmem<DIMS, TY, TZ> sm;
@@ -548,26 +568,8 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts,
   unsigned long long visits = 0;
   int cur_grid = -1, delta = 0;
   bool ok = true;
-  int pass = 0;
-  const unsigned long long t0 = jfc::global_ns();
-  unsigned long long t1 = t0;
-  {
-    BfsQ Q{ts.d_flag_bfs[1], ts.d_q_bfs[1], &ctr->qn_bfs[1]};
-    int wgrid = -1, wdelta = 0;
-    for (;;) {
-      const unsigned c = jfc::warp_ticket(&ctr->ticket[0]);
-      const long long b = (long long)c * 8;
-      if (b >= ts.ntiles) break;
-      const int cnt = (int)min(8ll, (long long)ts.ntiles - b);
-      for (int k = 0; k < cnt; ++k) {
-        relabel_first_warp<DIMS, TY, TZ>(ts, (int)b + k, Q, wgrid, wdelta);
-        ++visits;
-      }
-    }
-    if (lane == 0 && wdelta && wgrid >= 0) atomicAdd(&ts.d_grid_active[wgrid], wdelta);
-    ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
-    t1 = jfc::global_ns();
-  }
+  int pass = 1;
+  const unsigned long long t1 = jfc::global_ns();
   for (pass = 1; ok; ++pass) {
     const int cb = pass & 1;
     const int n = jfc::vload(&ctr->qn_bfs[cb]);
@@ -622,7 +624,7 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts,
     }
     ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
   }
-  // pass-0 visits were counted per warp (lane 0 of each), later ones by warp 0
+  // frontier visits are counted by warp 0 of each CTA; pass 0 visited every tile
   __shared__ unsigned long long s_vis;
   if (threadIdx.x == 0) s_vis = 0;
   __syncthreads();
@@ -632,9 +634,10 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts,
     if (s_vis) atomicAdd(&ctr->bfs_visits, s_vis);
     if (blockIdx.x == 0) {
       ctr->bfs_passes = pass;
+      ctr->bfs_visits += (unsigned long long)ts.ntiles;
       if (ctr->bfs_status == 0) ctr->bfs_status = 1;
       const unsigned long long t2 = jfc::global_ns();
-      ctr->ns_gr_first += t1 - t0;
+      ctr->ns_gr_first += t1 - ctr->t_gr_start;
       ctr->ns_gr_frontier += t2 - t1;
     }
   }
@@ -686,6 +689,13 @@ cudaError_t bfs_t(const TileSet& ts, int max_passes, cudaStream_t s) {
   const int nt = CUT ? 256 : RTile<DIMS, TY, TZ>::NT;
   static int blocks = 0;
   if (!blocks) blocks = persistent_blocks(fn, nt, 0);
+  if (!CUT) {
+    const long long fb = ((long long)ts.ntiles * 32 + 255) / 256;
+    jfc_note_launch();
+    k_relabel_first<DIMS, TY, TZ><<<(unsigned)fb, 256, 0, s>>>(ts);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   TileSet arg = ts;
   void* params[] = {(void*)&arg, (void*)&max_passes};
   jfc_note_launch();

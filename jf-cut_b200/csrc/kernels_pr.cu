@@ -250,6 +250,7 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
   __shared__ PrSmem<DIMS, TY, TZ> sm;
   DevCounters* ctr = ts.d_ctr;
   unsigned long long visits = 0, rounds = 0;
+  const unsigned long long t0 = jfc::global_ns();
   int s = 0;
   for (; s < 2 * sweeps; ++s) {
     const int p = s & 1;
@@ -281,7 +282,10 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
   if (threadIdx.x == 0) {
     if (visits) atomicAdd(&ctr->visits, visits);
     if (rounds) atomicAdd(&ctr->rounds, rounds);
-    if (blockIdx.x == 0) ctr->sweeps_done = s;
+    if (blockIdx.x == 0) {
+      ctr->sweeps_done = s;
+      ctr->ns_pr += jfc::global_ns() - t0;
+    }
   }
 }
 

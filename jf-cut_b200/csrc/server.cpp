@@ -329,7 +329,7 @@ void solver_loop(jfc_server* S) {
         if (rc) { fail_all(rc); return; }
       }
       int passes = 0, sw = 0;
-      int rc = engine_bfs(ctx, S->ts[k], p, false, passes, &active[k], nullptr, nullptr, &sw);
+      int rc = engine_bfs(ctx, S->ts[k], p, false, passes, &active[k], nullptr, &sw);
       if (rc) { fail_all(rc); return; }
       if (ran_pr[k])
         for (Member& m : mem[k]) m.s->sweeps += sw;

@@ -269,7 +269,7 @@ void jfc_default_params(jfc_params* out) {
   if (!out) return;
   std::memset(out, 0, sizeof(*out));
   fill_defaults(*out);
-  out->use_graph = 0;
+  out->use_graph = 1;
 }
 
 void jfc_default_model(jfc_model* out) {
@@ -305,6 +305,7 @@ int jfc_create(int device, const jfc_params* params, jfc_ctx** out) {
   jfc_ctx* c = new jfc_ctx();
   c->device = device;
   if (params) c->params = *params;
+  else jfc_default_params(&c->params);
   fill_defaults(c->params);
   e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete c; return cuda_status(e, "cudaStreamCreate"); }

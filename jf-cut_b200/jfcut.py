@@ -48,7 +48,7 @@ class Stats(ctypes.Structure):
                 ("source_nodes", ctypes.c_longlong), ("ms_total", ctypes.c_double), ("ms_build", ctypes.c_double),
                 ("ms_push_relabel", ctypes.c_double), ("ms_global_relabel", ctypes.c_double),
                 ("ms_cut", ctypes.c_double), ("pr_rounds", ctypes.c_longlong), ("bfs_visits", ctypes.c_longlong),
-                ("ms_gr_first", ctypes.c_double), ("ms_gr_frontier", ctypes.c_double)]
+                ("ms_gr_first", ctypes.c_double), ("ms_gr_frontier", ctypes.c_double), ("used_graph", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -62,6 +62,29 @@ def test_schedules_agree(ctx, tile_rows, local_iters, interval):
         ctx.set_params(tile_rows=16, local_iters=16, relabel_interval=8)
 
 
+def test_graph_replay_matches_direct_launches(ctx):
+    """Relabel cycles replayed from CUDA graphs give the same result as direct
+    launches, also when the cached graphs are reused by a second solve."""
+    shape, e, caps, published, _ = load_fixture("sponge")
+    results = []
+    try:
+        for use_graph in (0, 1, 1):
+            ctx.set_params(use_graph=use_graph, relabel_interval=2)
+            g, st = solve_set(ctx, shape, e, caps)
+            assert g.flow() == published
+            assert st.global_relabels > 1
+            assert st.used_graph == use_graph
+            results.append(g.labels().copy())
+            g2 = jfcut.Graph(ctx, shape)   # a second graph on the same context
+            g2.set(e, caps)
+            assert g2.solve().flow == published
+            g2.close()
+            g.close()
+    finally:
+        ctx.set_params(use_graph=1, relabel_interval=4)
+    assert all(np.array_equal(results[0], r) for r in results[1:])
+
+
 SHAPES = [(1, 1), (1, 37), (37, 1), (17, 33), (16, 32), (33, 65), (100, 1000), (257, 131),
           (1, 1, 1), (5, 5, 5), (3, 17, 9), (8, 33, 31), (13, 40, 70), (1, 1, 40), (40, 1, 1)]
 
@@ -220,6 +243,38 @@ def test_batch_matches_plain(ctx):
     for g, (e, caps, st) in zip(graphs, refs):
         check_against_oracle(g.shape, e, caps, g.flow(), g.labels(), sink_total=st)
     check_against_oracle(g3.shape, e3, c3, g3.flow(), g3.labels(), sink_total=st3)
+
+
+def test_batch_autotune_restores_and_matches(ctx):
+    rng = np.random.default_rng(21)
+    b = jfcut.Batch(ctx)
+    graphs, flows = [], []
+    for i in range(6):
+        w, h = int(rng.integers(40, 260)), int(rng.integers(40, 260))
+        img, seeds = jfcut.synth_rgb_ellipses(w, h, seed=700 + i)
+        g = jfcut.Graph(ctx, (h, w))
+        g.build_from_image(img, seeds, jfcut.PIX_RGB8, MODEL5)
+        ref = jfcut.Graph(ctx, (h, w))
+        ref.build_from_image(img, seeds, jfcut.PIX_RGB8, MODEL5)
+        ref.solve()
+        flows.append((ref.flow(), ref.labels().copy()))
+        ref.close()
+        graphs.append(g)
+        b.add(g)
+    base = ctx.params()
+    try:
+        p = b.autotune()
+        assert p.tile_rows in (8, 16) and p.local_iters in (8, 16, 32) and p.relabel_interval in (2, 4, 8, 16)
+        # the graphs are back in their built state: solving now gives the plain results
+        st = b.solve()
+        assert all(s.status == 0 for s in st)
+        for g, (f, lab) in zip(graphs, flows):
+            assert g.flow() == f
+            assert np.array_equal(g.labels(), lab)
+    finally:
+        ctx.set_params(tile_rows=base.tile_rows, local_iters=base.local_iters,
+                       relabel_interval=base.relabel_interval, relabel_interval_max=base.relabel_interval_max)
+    b.close()
 
 
 def test_errors(ctx):

@@ -369,7 +369,8 @@ def bench_edit4096(jfcut, torch, ctx, n_edits=30):
     return {"workload": "2D 4-conn RGB 4096x4096, %d sequential stroke edits (0.1-2%% of nodes)" % n_edits,
             "first_solve_ms": cold_first, "warm_p50_ms": pct(warm, 50), "warm_p99_ms": pct(warm, 99),
             "cold_resolve_p50_ms": pct(cold, 50), "cold_resolve_p99_ms": pct(cold, 99),
-            "cold_samples": len(cold), "bit_exact_vs_cold": bool(exact)}
+            "cold_samples": len(cold), "bit_exact_vs_cold": bool(exact),
+            "warm_ms": [round(v, 2) for v in warm]}
 
 
 def main():

@@ -186,7 +186,9 @@ int jfc_edit_tlinks(jfc_graph* g, const uint32_t* idx, const int32_t* dcs,
  * seed new_seed[j] (JFC_SEED_*) with the colour model kept fixed; the t-link
  * change is applied to the resident residual graph (the reference re-runs
  * slotModelClicked, QGCWidget.cpp:2560-2606, after every brush stroke,
- * QGCWidget.cpp:2243-2287).  Duplicate indices: the last one wins. */
+ * QGCWidget.cpp:2243-2287).  Duplicate indices: the last one wins.  The
+ * height plane serves as scratch until the next jfc_solve (which recomputes
+ * it), so jfc_graph_get_state reports meaningful heights only after a solve. */
 int jfc_graph_edit_seeds(jfc_graph* g, const uint32_t* idx, const uint8_t* new_seed, size_t n);
 
 /* Solve a 2D 4-connected grid without allocating anything.  No counterpart in

@@ -451,7 +451,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   JFC_CUDA(cudaEventRecord(ev[3], s));
   // device-clock phase times and visit counters
   unsigned long long* hv = (unsigned long long*)ctx->h_pin;
-  JFC_CUDA(cudaMemcpyAsync(hv, &ts.d_ctr->visits, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  JFC_CUDA(cudaMemcpyAsync(hv, &ts.d_ctr->visits, 15 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   JFC_CUDA(cudaEventRecord(ev[1], s));
   JFC_CUDA(cudaStreamSynchronize(s));
   st.ms_cut = elapsed_ms(ev[2], ev[3]);
@@ -463,6 +463,10 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   st.ms_gr_frontier = hv[4] * 1e-6;
   st.ms_global_relabel = st.ms_gr_first + st.ms_gr_frontier;
   st.ms_push_relabel = hv[5] * 1e-6;
+  if (p.verbose >= 2)   // phase-clock split (non-zero in JFC_PHASE_CLOCK builds)
+    fprintf(stderr, "{\"pr_cycles\": {\"stage\": %llu, \"local_relabel\": %llu, \"rounds\": %llu, \"exact_local\": %llu, "
+                    "\"write_back\": %llu, \"grid_barrier\": %llu}}\n",
+            hv[7], hv[8], hv[9], hv[12], hv[10], hv[11]);
   st.used_graph = graphs ? 1 : 0;
   for (int g = 0; g < ts.ngrids; ++g) {
     res[g].neg_sum = cut[g].neg_sum;

@@ -58,6 +58,7 @@ struct DevCounters {
   unsigned long long ns_gr_frontier;  // global relabel: frontier passes + queue refill
   unsigned long long ns_pr;           // push-relabel phases, device ns
   unsigned long long t_gr_start;      // device clock at the start of the last relabel
+  unsigned long long prof[8];         // SM-cycle split of push-relabel visits (JFC_PHASE_CLOCK builds)
 };
 
 // A set of grids tiled with one tile shape: the unit every launch works on

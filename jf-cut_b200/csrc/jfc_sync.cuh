@@ -52,6 +52,23 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
+// Phase-clock instrumentation (builds with -DJFC_PHASE_CLOCK): thread 0 adds
+// the SM cycles since `t` to counter k and restarts `t`.
+#ifdef JFC_PHASE_CLOCK
+#define JFC_PCLK_DECL long long _pclk = clock64();
+#define JFC_PCLK(ctr, k)                                                            \
+  do {                                                                              \
+    if (threadIdx.x == 0) {                                                         \
+      const long long _n = clock64();                                               \
+      atomicAdd(&(ctr)->prof[k], (unsigned long long)(_n - _pclk));                 \
+      _pclk = _n;                                                                   \
+    }                                                                               \
+  } while (0)
+#else
+#define JFC_PCLK_DECL
+#define JFC_PCLK(ctr, k) do {} while (0)
+#endif
+
 // Warp-cooperative append of up to 32 candidate tiles: lane k offers `tile`
 // when `want`; with `flags`, a tile is appended only by the lane that flips
 // its flag 0 -> 1 (so a queue never holds a tile twice).

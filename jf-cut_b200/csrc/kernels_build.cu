@@ -248,6 +248,26 @@ __global__ void __launch_bounds__(256) k_build(GridDev g, const void* __restrict
 
 // Warm stroke edit: re-seed nodes with the colour model fixed; the residual
 // graph stays, only e moves by the change of cs - ct (indices unique).
+// Duplicate indices in one edit list: the last entry of a node wins.  The
+// height plane is scratch between solves (every solve starts with a global
+// relabel that rewrites it), so it records the winning entry per node:
+// mark -1 on every edited node, then atomicMax of the entry index.
+__device__ __forceinline__ long long padded_of(const GridDev& g, long long i) {
+  const int x = (int)(i % g.W);
+  const long long yz = i / g.W;
+  const int y = (int)(yz % g.H), z = (int)(yz / g.H);
+  return (long long)x + (long long)g.pitch * (y + (long long)g.Hp * z);
+}
+
+__global__ void k_edit_mark(GridDev g, const uint32_t* __restrict__ idx, long long n, int last) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    int* h = g.h + padded_of(g, idx[j]);
+    if (last) atomicMax(h, (int)j);
+    else *h = -1;
+  }
+}
+
 template <int PF>
 __global__ void k_edit_seeds(GridDev g, const void* __restrict__ img, uint8_t* __restrict__ seeds,
                              BuildModelDev m, const int* __restrict__ lut_s, const int* __restrict__ lut_t,
@@ -257,6 +277,7 @@ __global__ void k_edit_seeds(GridDev g, const void* __restrict__ img, uint8_t* _
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
        j += (long long)gridDim.x * blockDim.x) {
     const long long i = idx[j];
+    if (g.h[padded_of(g, i)] != (int)j) continue;   // a later entry edits this node
     const int s1 = nseed[j], s0 = seeds[i];
     if (s0 == s1) continue;
     int f[3];
@@ -359,6 +380,9 @@ cudaError_t launch_edit_seeds(const GridDev& g, const void* d_img, uint8_t* d_se
                               const uint8_t* d_new, size_t n, long long* d_dsink, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   const int nb = flat_blocks((long long)n);
+  jfc_note_launch(2);
+  k_edit_mark<<<nb, 256, 0, s>>>(g, d_idx, (long long)n, 0);
+  k_edit_mark<<<nb, 256, 0, s>>>(g, d_idx, (long long)n, 1);
   switch (m.pixfmt) {
     case JFC_PIX_GRAY8:
       jfc_note_launch();

@@ -29,6 +29,11 @@
 #include "jfc_relax.cuh"
 
 
+// Iteration cap of the exact local relabel at the start of a visit (0: none).
+#ifndef JFC_LOCAL_RELABEL_ITERS
+#define JFC_LOCAL_RELABEL_ITERS 8
+#endif
+
 namespace {
 
 using jfc::FULL;
@@ -67,6 +72,7 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
   const long long tbase = (long long)x0 + (long long)y0 * pitch + (long long)z0 * slab;
   const long long n = tbase + x + (long long)y * pitch + (long long)z * slab;
   const int hi = T::hidx(x, y, z);
+  JFC_PCLK_DECL
 
   // ---- stage the tile and its halo heights
   const int e0 = g.e[n], h0 = g.h[n];
@@ -107,13 +113,20 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
     s.h[hi] = e0 < 0 ? 0 : JFC_INF;
   }
   __syncthreads();
-  {
+  JFC_PCLK(ts.d_ctr, 0);
+  if (JFC_LOCAL_RELABEL_ITERS > 0) {
     // a partial relaxation overestimates distances, so the local labelling
     // is only applied when the in-tile fixpoint was reached
-    const bool exact = jfc::relax_cta<DIMS, TY, TZ>(s.h, s.arc, 8);
+    const bool exact = jfc::relax_cta<DIMS, TY, TZ>(s.h, s.arc, JFC_LOCAL_RELABEL_ITERS);
     s.h[hi] = exact ? max(s.h[hi], h0) : h0;
+#ifdef JFC_PHASE_CLOCK
+    if (threadIdx.x == 0 && exact) atomicAdd(&ts.d_ctr->prof[5], 1ull);
+#endif
+  } else {
+    s.h[hi] = h0;
   }
   __syncthreads();
+  JFC_PCLK(ts.d_ctr, 1);
 
   // in-tile neighbours, or the halo cell a push across the border lands in
   const bool in_xp = x < 31, in_xm = x > 0, in_yp = y < TY - 1, in_ym = y > 0;
@@ -191,6 +204,7 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
     if (!__syncthreads_or(did)) break;
   }
   const int rounds = it < local_iters ? it + 1 : local_iters;
+  JFC_PCLK(ts.d_ctr, 2);
 
   // ---- write back the words that changed
   const int e1 = s.e[t], h1 = s.h[hi];
@@ -237,6 +251,7 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
     jfc::warp_append(active && t == 0, tid, nullptr, self_q, self_n);
   }
   __syncthreads();
+  JFC_PCLK(ts.d_ctr, 3);
   return rounds;
 }
 
@@ -272,11 +287,13 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
                                        ts.d_q_pr[p ^ 1][bo], &ctr->qn_pr[p ^ 1][bo]);
       ++visits;
     }
+    JFC_PCLK_DECL
     const bool ok = jfc::grid_sync(ctr, [&]() {
       ctr->ticket[s & 1] = 0;
       ctr->qn_pr[p][b] = 0;
       ctr->cur_pr[p] = b ^ 1;
     });
+    JFC_PCLK(ctr, 4);
     if (!ok) break;
   }
   if (threadIdx.x == 0) {

@@ -528,20 +528,12 @@ int jfc_graph_edit_seeds(jfc_graph* G, const uint32_t* idx, const uint8_t* new_s
   if (!G || (n && (!idx || !new_seed))) return set_error(JFC_ERR_INVALID_ARG, "null argument");
   if (!G->model.valid) return set_error(JFC_ERR_STATE, "graph was not built from an image");
   const unsigned long long N = (unsigned long long)G->W * G->H * G->D;
-  // unique indices (last edit of a node wins)
-  std::unordered_map<uint32_t, uint8_t> last;
-  last.reserve(n * 2);
-  for (size_t j = 0; j < n; ++j) {
+  for (size_t j = 0; j < n; ++j)
     if (idx[j] >= N || new_seed[j] > 2) return set_error(JFC_ERR_INVALID_ARG, "bad edit");
-    last[idx[j]] = new_seed[j];
-  }
-  if (last.empty()) return JFC_OK;
-  std::vector<uint32_t> ui;
-  std::vector<uint8_t> us;
-  ui.reserve(last.size());
-  us.reserve(last.size());
-  for (auto& kv : last) { ui.push_back(kv.first); us.push_back(kv.second); }
-  const size_t m = ui.size();
+  if (n == 0) return JFC_OK;
+  if (n > (size_t)0x7fffffff) return set_error(JFC_ERR_INVALID_ARG, "edit list too long");
+  // duplicates are resolved on the device (the last entry of a node wins)
+  const size_t m = n;
   JFC_CUDA(cudaSetDevice(G->ctx->device));
   cudaStream_t s = G->ctx->stream;
   char* buf = nullptr;
@@ -549,8 +541,8 @@ int jfc_graph_edit_seeds(jfc_graph* G, const uint32_t* idx, const uint8_t* new_s
   uint32_t* d_idx = (uint32_t*)buf;
   uint8_t* d_new = (uint8_t*)(buf + align256(m * 4));
   long long* d_ds = (long long*)(buf + align256(m * 4) + align256(m));
-  cudaError_t e = cudaMemcpyAsync(d_idx, ui.data(), m * 4, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(d_new, us.data(), m, cudaMemcpyHostToDevice, s);
+  cudaError_t e = cudaMemcpyAsync(d_idx, idx, m * 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_new, new_seed, m, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_ds, 0, sizeof(long long), s);
   if (e == cudaSuccess)
     e = launch_edit_seeds(G->g, G->model.d_img, G->model.d_seeds, G->model.m, G->model.d_lut_s,

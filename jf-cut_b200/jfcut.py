@@ -15,7 +15,8 @@ import weakref
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libjfcut.so")
+# JFCUT_LIB selects another build of the library (e.g. an instrumented one)
+LIB_PATH = os.environ.get("JFCUT_LIB") or os.path.join(HERE, "libjfcut.so")
 
 OK, ERR_INVALID_ARG, ERR_NO_SEEDS, ERR_OOM, ERR_NOT_CONVERGED, ERR_CUDA, ERR_NO_DEVICE, ERR_STATE, \
     ERR_CANCELLED, ERR_BUSY = range(10)

@@ -196,6 +196,31 @@ def test_warm_seed_edits(ctx):
         cold.close()
 
 
+def test_seed_edit_duplicates_last_wins(ctx):
+    img, seeds = jfcut.synth_rgb_ellipses(160, 120, seed=12)
+    rng = np.random.default_rng(4)
+    n = seeds.size
+    idx = rng.integers(0, n, 3000).astype(np.uint32)          # many repeated nodes
+    ns = rng.integers(0, 3, 3000).astype(np.uint8)
+    last = {}
+    for i, v in zip(idx.tolist(), ns.tolist()):
+        last[i] = v
+    ui = np.array(sorted(last), np.uint32)
+    us = np.array([last[i] for i in ui.tolist()], np.uint8)
+    out = []
+    for a, b in ((idx, ns), (ui, us)):
+        g = jfcut.Graph(ctx, seeds.shape)
+        g.build_from_image(img, seeds, jfcut.PIX_RGB8, MODEL5)
+        g.solve()
+        g.edit_seeds(a, b)
+        g.solve()
+        out.append((g.flow(), g.labels().copy(), g.state()[0].copy()))
+        g.close()
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
+
+
 def test_edit_tlinks_deltas(ctx):
     rng = np.random.default_rng(3)
     shape = (70, 90)

@@ -248,6 +248,44 @@ def bench_batched(jfcut, torch, ctx, stream, steps, warmup, n_inst=256):
     return out
 
 
+def bench_video(jfcut, torch, ctx, stream, steps=2, warmup=1):
+    """3D plain workload: 6-connected 2560x1440x50 RGB video (184M nodes), an
+    ellipse moving 4 px/frame over seeded value-noise texture, temporal n-link
+    weight 0.5x the spatial one, 5-means colour models, strokes on frames 0
+    and 49.  One step = capacity build from device-resident frames + solve +
+    labels into a device buffer; flows must repeat exactly."""
+    w, h, d = 2560, 1440, 50
+    img, seeds = jfcut.synth_rgb_video(w, h, d, seed=SEED + 50)
+    model = dict(MODEL, z_weight_pct=50)
+    d_img = torch.from_numpy(img).cuda()
+    d_seeds = torch.from_numpy(seeds).cuda()
+    d_lab = torch.empty(w * h * d, dtype=torch.uint8, device="cuda")
+    g = jfcut.Graph(ctx, (d, h, w))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms, flows, agg = [], set(), None
+    for it in range(warmup + steps):
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        g.build_from_device(d_img.data_ptr(), d_seeds.data_ptr(), jfcut.PIX_RGB8, model)
+        st = g.solve()
+        g.read_labels_device(d_lab.data_ptr())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        flows.add(g.flow())
+        if it >= warmup:
+            ms.append(ev0.elapsed_time(ev1))
+            agg = st
+    g.close()
+    n = w * h * d
+    m = float(np.mean(ms))
+    return {"workload": "3D 6-conn 2560x1440x50 RGB video (build + solve + labels per step)", "nodes": n,
+            "ms_per_step": m, "mnodes_s": n / (m / 1e3) / 1e6, "flow": flows.pop() if len(flows) == 1 else None,
+            "flow_repeatable": len(flows) <= 1,
+            "solve_breakdown": {k: round(getattr(agg, k), 2) for k in
+                                ("ms_total", "ms_push_relabel", "ms_global_relabel", "ms_cut", "sweeps",
+                                 "global_relabels")}}
+
+
 def bench_serve(jfcut, torch, ctx, n_req=48, rate=200.0, budget_gb=96):
     """Serving workload: Poisson arrivals (mean `rate`/s) of n_req sessions,
     70% 2D RGB images (sides U[256,4096], 4-conn) and 30% int16 phantom
@@ -382,8 +420,8 @@ def main():
     ap.add_argument("--width", type=int, default=W_FULL)
     ap.add_argument("--height", type=int, default=H_FULL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--extras", default="batched,serve,edit4096",
-                    help="comma list of extra sections at N=1 (batched, serve, edit4096) or 'none'")
+    ap.add_argument("--extras", default="video,batched,edit4096,serve",
+                    help="comma list of extra sections at N=1 (video, batched, edit4096, serve) or 'none'")
     ap.add_argument("--serve-requests", type=int, default=48)
     args = ap.parse_args()
     if args.impl == "reference":
@@ -515,11 +553,12 @@ def main():
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_bk()
         extras = [] if world > 1 or args.extras == "none" else args.extras.split(",")
-        sections = {"batched": lambda: bench_batched(jfcut, torch, ctx, stream, 2, 1),
+        sections = {"video": lambda: bench_video(jfcut, torch, ctx, stream),
+                    "batched": lambda: bench_batched(jfcut, torch, ctx, stream, 2, 1),
                     "edit4096": lambda: bench_edit4096(jfcut, torch, ctx),
                     "serve": lambda: bench_serve(jfcut, torch, ctx, n_req=args.serve_requests)}
         with torch.cuda.stream(stream):
-            for name in ("batched", "edit4096", "serve"):
+            for name in ("video", "batched", "edit4096", "serve"):
                 if name in extras:
                     t0 = time.perf_counter()
                     try:

@@ -53,7 +53,8 @@ enum {
   JFC_ERR_NO_DEVICE = 6,     /* no CUDA device / extension cannot run here */
   JFC_ERR_STATE = 7,         /* call out of order (e.g. labels before solve) */
   JFC_ERR_CANCELLED = 8,     /* server request cancelled */
-  JFC_ERR_BUSY = 9           /* server queue full / request not finished */
+  JFC_ERR_BUSY = 9,          /* server queue full / request not finished */
+  JFC_ERR_IO = 10            /* a data file could not be opened, read or written */
 };
 
 /* Pixel formats of jfc_graph_build_from_image (the reference reads a float
@@ -255,6 +256,62 @@ typedef struct jfc_server_stats {
   int64_t loops, requests_done;
 } jfc_server_stats;
 int  jfc_server_get_stats(jfc_server* s, jfc_server_stats* out);
+
+/* Energy of a labelling over a graph given as dense device arrays (the
+ * reference's energy check after a solve, QGCWidget.cpp:2452-2520):
+ * data = sum over background nodes of max(e, 0) + sum over object nodes of
+ * max(-e, 0); smooth = sum of the capacities of arcs from object to background
+ * nodes.  With the original capacities and the canonical cut, data + smooth
+ * equals the (net-excess) max-flow: an independent certificate.  stream is a
+ * cudaStream_t (NULL = legacy default stream). */
+int jfc_energy_device(int device, void* stream, int dims, int w, int h, int d, const int32_t* d_excess,
+                      const int32_t* const* d_ncap, const uint8_t* d_labels, int64_t* data, int64_t* smooth);
+
+/* ---- the reference's data files (host only; no device work) ----
+ * Dense arrays (w*h*d, x fastest) in the solver's channel order. */
+enum { JFC_FMT_UCHAR = 0, JFC_FMT_CHAR, JFC_FMT_USHORT, JFC_FMT_SHORT, JFC_FMT_UINT, JFC_FMT_INT, JFC_FMT_FLOAT };
+typedef struct jfc_volume_info {
+  char object_file[256];     /* "Object File Name" (the .raw next to the header) */
+  int w, h, d;               /* "Resolution" */
+  float thickness[3];        /* "Slice Thickness" */
+  int format;                /* JFC_FMT_* ("Format") */
+  int big_endian;            /* "Endian" */
+  float intensity_min, intensity_max;  /* "Intensity Extremums" */
+} jfc_volume_info;
+/* .dat volume header (QGCWidget::parseDataFile / saveDataFile, QGCWidget.cpp:296-683). */
+int jfc_read_dat(const char* path, jfc_volume_info* out);
+int jfc_write_dat(const char* path, const jfc_volume_info* info);
+/* .raw samples in the header's format and endianness, widened to float. */
+int jfc_read_raw(const char* path, const jfc_volume_info* info, float* out);
+/* <base>.ef / .c1 / .c2 graph files (slotLoadGraphClicked / slotSaveGraphClicked,
+ * QGCWidget.cpp:2631-2736): int32 net excess; 2D ushort2 (+x, +y), (-y, -x);
+ * 3D uchar4 (+x, +y, +z, -), (-z, -y, -x, -).  ncap[conn] receive / give the
+ * capacities; saving rejects capacities that do not fit the file's type. */
+int jfc_load_graph_files(const char* base, int dims, int w, int h, int d, int32_t* excess, int32_t* const* ncap);
+int jfc_save_graph_files(const char* base, int dims, int w, int h, int d, const int32_t* excess,
+                         const int32_t* const* ncap);
+/* .cut: 4 bytes per node {foreground seed, background seed, object, tag}
+ * (cl_cut, QGCSetting.h:46-51).  seeds in JFC_SEED_*, labels 1 = object;
+ * either pointer may be NULL. */
+int jfc_read_cut(const char* path, size_t n, uint8_t* seeds, uint8_t* labels);
+int jfc_write_cut(const char* path, size_t n, const uint8_t* seeds, const uint8_t* labels);
+/* .mfi max-flow instances of the GridCut benchmark (3rdParty/bench/mfi.cpp,
+ * QGCWidget::saveMFI, QGCWidget.cpp:3339-3474), 2D/4 and 3D/6 only. */
+typedef struct jfc_mfi_info {
+  int dims, conn, w, h, d;
+  int64_t maxflow;           /* the file's recorded max-flow */
+  int active_count;
+  int type_terminal, type_neighbor;   /* 0 uint8, 1 uint16, 2 uint32 */
+} jfc_mfi_info;
+int jfc_read_mfi_info(const char* path, jfc_mfi_info* out);
+/* Net excess e = cs - ct, neighbour capacities, *flow_offset = sum min(cs, ct)
+ * (pass it to jfc_graph_set); mask (n bytes) may be NULL. */
+int jfc_load_mfi(const char* path, int32_t* excess, int32_t* const* ncap, int64_t* flow_offset, uint8_t* mask);
+/* Terminal caps as max(e, 0) / max(-e, 0) in uint32 (as the reference writes
+ * them); neighbour caps uint16 (2D) / uint8 (3D), or uint32 when one does
+ * not fit; mask may be NULL (zeros). */
+int jfc_save_mfi(const char* path, int dims, int w, int h, int d, const int32_t* excess, const int32_t* const* ncap,
+                 int64_t maxflow, const uint8_t* mask);
 
 /* ---- synthetic inputs (seeded, deterministic, integer arithmetic) used by the
  * tests and the benchmark in place of the reference's image files ---- */

@@ -150,7 +150,11 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDe
     ts.d_block = blk;
     ts.block_bytes = total;
     tileset_carve(ts, blk, &total);
-    JFC_CUDA(cudaMemset(blk, 0, total));
+    // on the caller's stream when staging asynchronously: the table uploads
+    // below are ordered after it (a legacy-stream memset is not ordered with a
+    // non-blocking stream)
+    if (s) JFC_CUDA(cudaMemsetAsync(blk, 0, total, s));
+    else JFC_CUDA(cudaMemset(blk, 0, total));
   }
   tileset_drop_graphs(ts);   // captured launches hold the old tile set by value
   ts.dims = dims;

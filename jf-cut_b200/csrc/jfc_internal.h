@@ -87,6 +87,11 @@ struct TileSet {
   void* gcache = nullptr;            // captured relabel-cycle graphs (engine.cpp)
 };
 
+// (kernels_post.cu) labelling energy over dense device arrays: out[0] data,
+// out[1] smooth (int64 sums, out zeroed by the caller)
+cudaError_t launch_energy(int dims, int w, int h, int d, const int32_t* e, const int32_t* const* caps,
+                          const uint8_t* lab, unsigned long long* out, cudaStream_t s);
+
 // Counts every kernel launch of the library (engine.cpp).
 void jfc_note_launch(int n = 1);
 

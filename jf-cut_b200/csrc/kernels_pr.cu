@@ -59,8 +59,8 @@ __device__ __forceinline__ void halo_cell(int c, int& x, int& y, int& z, int& fa
 }
 
 template <int DIMS, int TY, int TZ>
-__device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_iters, PrSmem<DIMS, TY, TZ>& s,
-                                        int* self_q, int* self_n, int* nbr_q, int* nbr_n) {
+__device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_iters, bool local_relabel,
+                                        PrSmem<DIMS, TY, TZ>& s, int* self_q, int* self_n, int* nbr_q, int* nbr_n) {
   using T = Tile<DIMS, TY, TZ>;
   const int t = threadIdx.x;
   const int x = t & 31, row = t >> 5, y = row % TY, z = row / TY;
@@ -114,7 +114,7 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
   }
   __syncthreads();
   JFC_PCLK(ts.d_ctr, 0);
-  if (JFC_LOCAL_RELABEL_ITERS > 0) {
+  if (JFC_LOCAL_RELABEL_ITERS > 0 && local_relabel) {
     // a partial relaxation overestimates distances, so the local labelling
     // is only applied when the in-tile fixpoint was reached
     const bool exact = jfc::relax_cta<DIMS, TY, TZ>(s.h, s.arc, JFC_LOCAL_RELABEL_ITERS);
@@ -166,36 +166,50 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
       }
       __syncthreads();
     }
-    // push: every node with excess, along admissible arcs in reference order
+    // push: every node with excess, along admissible arcs in reference order.
+    // All operands are loaded first and the pushes are computed in registers,
+    // then issued as independent shared-memory updates: a push u->v needs
+    // h(u) = h(v) + 1, so in one step nothing else writes u's own arcs or the
+    // reverse arc v->u that u credits (the credits are reductions, no load).
     {
       const int h = s.h[hi];
       const int e = s.e[t];
       if (e > 0 && h < JFC_INF) {
         const int hm = h - 1;
+        constexpr int NP = DIMS == 3 ? 6 : 4;
+        // push order: +x, +y, -y, (+z, -z,) -x; q is a constant after unrolling
+        auto slot = [](int q) { return q == 0 ? T::XP : q == 1 ? T::YP : q == 2 ? T::YM
+                                              : q == NP - 1 ? T::XM : q == 3 ? T::ZP : T::ZM; };
+        auto hoff = [](int q) { return q == 0 ? 1 : q == 1 ? T::HX : q == 2 ? -T::HX
+                                             : q == NP - 1 ? -1 : q == 3 ? T::HX * T::HY : -T::HX * T::HY; };
+        auto toff = [](int q) { return q == 0 ? 1 : q == 1 ? 32 : q == 2 ? -32
+                                             : q == NP - 1 ? -1 : q == 3 ? 32 * TY : -32 * TY; };
+        const bool inside[6] = {in_xp, in_yp, in_ym, DIMS == 3 ? in_zp : in_xm, in_zm, in_xm};
+        const int hcell[6] = {hc_xp, hc_yp, hc_ym, DIMS == 3 ? hc_zp : hc_xm, hc_zm, hc_xm};
+        int hn[NP], rk[NP], d[NP];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) hn[q] = s.h[hi + hoff(q)];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) rk[q] = s.r[slot(q)][t];
         int ex = e;
-        auto push = [&](int k, int rev, int hn, bool inside, int tn, int hc) {
-          const int rk = s.r[k][t];
-          if (ex > 0 && rk > 0 && hn == hm) {
-            const int d = min(ex, rk);
-            s.r[k][t] = rk - d;
-            ex -= d;
-            if (inside) {
-              atomicAdd(&s.e[tn], d);
-              s.r[rev][tn] += d;
-            } else {
-              s.out[hc] += d;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+          d[q] = (ex > 0 && rk[q] > 0 && hn[q] == hm) ? min(ex, rk[q]) : 0;
+          ex -= d[q];
+        }
+        if (ex != e) {
+#pragma unroll
+          for (int q = 0; q < NP; ++q) {
+            if (d[q]) {
+              s.r[slot(q)][t] = rk[q] - d[q];
+              if (inside[q == NP - 1 ? 5 : q]) {
+                atomicAdd(&s.e[t + toff(q)], d[q]);
+                atomicAdd(&s.r[T::K - 1 - slot(q)][t + toff(q)], d[q]);
+              } else {
+                s.out[hcell[q == NP - 1 ? 5 : q]] += d[q];
+              }
             }
           }
-        };
-        push(T::XP, T::XM, s.h[hi + 1], in_xp, t + 1, hc_xp);
-        push(T::YP, T::YM, s.h[hi + T::HX], in_yp, t + 32, hc_yp);
-        push(T::YM, T::YP, s.h[hi - T::HX], in_ym, t - 32, hc_ym);
-        if constexpr (DIMS == 3) {
-          push(T::ZP, T::ZM, s.h[hi + T::HX * T::HY], in_zp, t + 32 * TY, hc_zp);
-          push(T::ZM, T::ZP, s.h[hi - T::HX * T::HY], in_zm, t - 32 * TY, hc_zm);
-        }
-        push(T::XM, T::XP, s.h[hi - 1], in_xm, t - 1, hc_xm);
-        if (ex != e) {
           atomicAdd(&s.e[t], ex - e);
           did = true;
         }
@@ -283,7 +297,10 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
       __syncthreads();
       const int tid = sm.tile;
       if (tid < 0) break;
-      rounds += pr_visit<DIMS, TY, TZ>(ts, tid, local_iters, sm, ts.d_q_pr[p][b ^ 1], &ctr->qn_pr[p][b ^ 1],
+      // first sweep of a phase: nothing moved since the exact global relabel
+      // (the halo tiles have the other parity), so the local relabel would
+      // reproduce the heights it finds
+      rounds += pr_visit<DIMS, TY, TZ>(ts, tid, local_iters, s > 0, sm, ts.d_q_pr[p][b ^ 1], &ctr->qn_pr[p][b ^ 1],
                                        ts.d_q_pr[p ^ 1][bo], &ctr->qn_pr[p ^ 1][bo]);
       ++visits;
     }

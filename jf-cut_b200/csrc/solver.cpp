@@ -290,6 +290,7 @@ const char* jfc_strerror(int status) {
     case JFC_ERR_STATE: return "call out of order";
     case JFC_ERR_CANCELLED: return "request cancelled";
     case JFC_ERR_BUSY: return "busy";
+    case JFC_ERR_IO: return "data file I/O error";
     default: return "unknown status";
   }
 }
@@ -521,6 +522,29 @@ int jfc_edit_tlinks(jfc_graph* G, const uint32_t* idx, const int32_t* dcs, const
   if (e != cudaSuccess) return cuda_status(e, "edit t-links");
   G->sink_total += ds;
   G->state = 1;
+  return JFC_OK;
+}
+
+int jfc_energy_device(int device, void* stream, int dims, int w, int h, int d, const int32_t* d_excess,
+                      const int32_t* const* d_ncap, const uint8_t* d_labels, int64_t* data, int64_t* smooth) {
+  if (!d_excess || !d_ncap || !d_labels || !data || !smooth) return set_error(JFC_ERR_INVALID_ARG, "null argument");
+  if (dims == 2) d = 1;
+  if ((dims != 2 && dims != 3) || w < 1 || h < 1 || d < 1) return set_error(JFC_ERR_INVALID_ARG, "bad grid shape");
+  for (int k = 0; k < (dims == 3 ? 6 : 4); ++k)
+    if (!d_ncap[k]) return set_error(JFC_ERR_INVALID_ARG, "null capacity array");
+  JFC_CUDA(cudaSetDevice(device));
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned long long* d_out = nullptr;
+  JFC_CUDA(cudaMallocAsync((void**)&d_out, 2 * sizeof(unsigned long long), s));
+  unsigned long long h_out[2] = {0, 0};
+  cudaError_t e = cudaMemsetAsync(d_out, 0, sizeof(h_out), s);
+  if (e == cudaSuccess) e = launch_energy(dims, w, h, d, d_excess, d_ncap, d_labels, d_out, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h_out, d_out, sizeof(h_out), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFreeAsync(d_out, s);
+  if (e != cudaSuccess) return cuda_status(e, "energy");
+  *data = (int64_t)h_out[0];
+  *smooth = (int64_t)h_out[1];
   return JFC_OK;
 }
 

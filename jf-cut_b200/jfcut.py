@@ -19,7 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("JFCUT_LIB") or os.path.join(HERE, "libjfcut.so")
 
 OK, ERR_INVALID_ARG, ERR_NO_SEEDS, ERR_OOM, ERR_NOT_CONVERGED, ERR_CUDA, ERR_NO_DEVICE, ERR_STATE, \
-    ERR_CANCELLED, ERR_BUSY = range(10)
+    ERR_CANCELLED, ERR_BUSY, ERR_IO = range(11)
+FMT_UCHAR, FMT_CHAR, FMT_USHORT, FMT_SHORT, FMT_UINT, FMT_INT, FMT_FLOAT = range(7)
 PIX_GRAY8, PIX_RGB8, PIX_I16 = 0, 1, 2
 SEED_NONE, SEED_FG, SEED_BG = 0, 1, 2
 
@@ -67,6 +68,22 @@ class ServerStats(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class VolumeInfo(ctypes.Structure):
+    _fields_ = [("object_file", ctypes.c_char * 256), ("w", ctypes.c_int), ("h", ctypes.c_int), ("d", ctypes.c_int),
+                ("thickness", ctypes.c_float * 3), ("format", ctypes.c_int), ("big_endian", ctypes.c_int),
+                ("intensity_min", ctypes.c_float), ("intensity_max", ctypes.c_float)]
+
+
+class MfiInfo(ctypes.Structure):
+    _fields_ = [("dims", ctypes.c_int), ("conn", ctypes.c_int), ("w", ctypes.c_int), ("h", ctypes.c_int),
+                ("d", ctypes.c_int), ("maxflow", ctypes.c_int64), ("active_count", ctypes.c_int),
+                ("type_terminal", ctypes.c_int), ("type_neighbor", ctypes.c_int)]
+
+    @property
+    def shape(self):
+        return (self.h, self.w) if self.dims == 2 else (self.d, self.h, self.w)
 
 
 _LIB = None
@@ -134,6 +151,20 @@ def _lib():
         L.jfc_server_close.argtypes = [VP, ctypes.c_int]
         L.jfc_server_cancel.argtypes = [VP, ctypes.c_int]
         L.jfc_server_get_stats.argtypes = [VP, ctypes.POINTER(ServerStats)]
+        L.jfc_energy_device.argtypes = [ctypes.c_int, VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        VP, ctypes.POINTER(VP), VP, ctypes.POINTER(ctypes.c_int64),
+                                        ctypes.POINTER(ctypes.c_int64)]
+        CP = ctypes.c_char_p
+        L.jfc_read_dat.argtypes = [CP, ctypes.POINTER(VolumeInfo)]
+        L.jfc_write_dat.argtypes = [CP, ctypes.POINTER(VolumeInfo)]
+        L.jfc_read_raw.argtypes = [CP, ctypes.POINTER(VolumeInfo), ctypes.POINTER(ctypes.c_float)]
+        L.jfc_load_graph_files.argtypes = [CP] + [ctypes.c_int] * 4 + [I32P, ctypes.POINTER(I32P)]
+        L.jfc_save_graph_files.argtypes = [CP] + [ctypes.c_int] * 4 + [I32P, ctypes.POINTER(I32P)]
+        L.jfc_read_cut.argtypes = [CP, ctypes.c_size_t, U8P, U8P]
+        L.jfc_write_cut.argtypes = [CP, ctypes.c_size_t, U8P, U8P]
+        L.jfc_read_mfi_info.argtypes = [CP, ctypes.POINTER(MfiInfo)]
+        L.jfc_load_mfi.argtypes = [CP, I32P, ctypes.POINTER(I32P), ctypes.POINTER(ctypes.c_int64), U8P]
+        L.jfc_save_mfi.argtypes = [CP] + [ctypes.c_int] * 4 + [I32P, ctypes.POINTER(I32P), ctypes.c_int64, U8P]
         L.jfc_synth_gray_ellipse.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int, U8P, U8P]
         L.jfc_synth_rgb_ellipses.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
                                              ctypes.c_int, ctypes.c_int, U8P, U8P]
@@ -269,6 +300,19 @@ class Graph:
         _check(_lib().jfc_graph_set(self.handle, _p(e, I32P), P, int(flow_offset)), "jfc_graph_set")
 
     slotLoadGraphClicked = set
+
+    def load_files(self, base):
+        """Load <base>.ef/.c1/.c2 (the reference's graph files) into this grid."""
+        e, caps = load_graph_files(base, self.shape)
+        self.set(e, caps, 0)
+
+    def load_mfi(self, path):
+        """Load a GridCut-benchmark .mfi instance; returns its recorded max-flow."""
+        info, e, caps, off, _ = load_mfi(path)
+        if tuple(info.shape) != tuple(self.shape):
+            raise ValueError("MFI shape %s does not match the grid %s" % (info.shape, self.shape))
+        self.set(e, caps, off)
+        return info.maxflow
 
     def set_device(self, d_excess, d_caps, flow_offset=0):
         P = (VP * self.conn)(*[VP(p) for p in d_caps])
@@ -450,6 +494,113 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def energy_device(device, shape, d_excess, d_caps, d_labels, stream=0):
+    """Energy (data, smooth) of a labelling over dense device arrays (int
+    pointers): the reference's post-solve energy check."""
+    dims, w, h, d = _dims(shape)
+    data, smooth = ctypes.c_int64(0), ctypes.c_int64(0)
+    P = (VP * len(d_caps))(*[VP(p) for p in d_caps])
+    _check(_lib().jfc_energy_device(int(device), VP(stream or None), dims, w, h, d, VP(d_excess), P, VP(d_labels),
+                                    ctypes.byref(data), ctypes.byref(smooth)), "jfc_energy_device")
+    return data.value, smooth.value
+
+
+# ---------------------------------------------------------------- data files
+def _dims(shape):
+    if len(shape) == 2:
+        return 2, int(shape[1]), int(shape[0]), 1
+    return 3, int(shape[2]), int(shape[1]), int(shape[0])
+
+
+def _b(path):
+    return os.fsencode(path)
+
+
+def read_dat(path):
+    """Volume header (.dat) -> VolumeInfo."""
+    info = VolumeInfo()
+    _check(_lib().jfc_read_dat(_b(path), ctypes.byref(info)), "jfc_read_dat")
+    return info
+
+
+def write_dat(path, info):
+    _check(_lib().jfc_write_dat(_b(path), ctypes.byref(info)), "jfc_write_dat")
+
+
+def read_raw(path, info):
+    """Samples of a .raw volume as float32, shape (h, w) or (d, h, w)."""
+    out = np.empty(info.w * info.h * info.d, np.float32)
+    _check(_lib().jfc_read_raw(_b(path), ctypes.byref(info), out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+           "jfc_read_raw")
+    return out.reshape((info.h, info.w) if info.d == 1 else (info.d, info.h, info.w))
+
+
+def load_graph_files(base, shape):
+    """<base>.ef/.c1/.c2 -> (excess, caps) in the solver's channel order."""
+    dims, w, h, d = _dims(shape)
+    n = w * h * d
+    e = np.empty(n, np.int32)
+    caps = [np.empty(n, np.int32) for _ in range(4 if dims == 2 else 6)]
+    P = (I32P * len(caps))(*[_p(c, I32P) for c in caps])
+    _check(_lib().jfc_load_graph_files(_b(base), dims, w, h, d, _p(e, I32P), P), "jfc_load_graph_files")
+    return e.reshape(shape), [c.reshape(shape) for c in caps]
+
+
+def save_graph_files(base, excess, caps):
+    dims, w, h, d = _dims(np.shape(excess))
+    e = np.ascontiguousarray(excess, np.int32).ravel()
+    cs = [np.ascontiguousarray(c, np.int32).ravel() for c in caps]
+    P = (I32P * len(cs))(*[_p(c, I32P) for c in cs])
+    _check(_lib().jfc_save_graph_files(_b(base), dims, w, h, d, _p(e, I32P), P), "jfc_save_graph_files")
+
+
+def read_cut(path, shape):
+    """.cut -> (seeds JFC_SEED_*, labels 1 = object)."""
+    n = int(np.prod(shape))
+    seeds = np.empty(n, np.uint8)
+    labels = np.empty(n, np.uint8)
+    _check(_lib().jfc_read_cut(_b(path), n, _p(seeds, U8P), _p(labels, U8P)), "jfc_read_cut")
+    return seeds.reshape(shape), labels.reshape(shape)
+
+
+def write_cut(path, seeds, labels):
+    s_ = None if seeds is None else np.ascontiguousarray(seeds, np.uint8).ravel()
+    l_ = None if labels is None else np.ascontiguousarray(labels, np.uint8).ravel()
+    n = (s_ if s_ is not None else l_).size
+    _check(_lib().jfc_write_cut(_b(path), n, None if s_ is None else _p(s_, U8P),
+                                None if l_ is None else _p(l_, U8P)), "jfc_write_cut")
+
+
+def read_mfi_info(path):
+    info = MfiInfo()
+    _check(_lib().jfc_read_mfi_info(_b(path), ctypes.byref(info)), "jfc_read_mfi_info")
+    return info
+
+
+def load_mfi(path):
+    """.mfi -> (info, excess, caps, flow_offset, mask)."""
+    info = read_mfi_info(path)
+    shape = info.shape
+    n = int(np.prod(shape))
+    e = np.empty(n, np.int32)
+    caps = [np.empty(n, np.int32) for _ in range(info.conn)]
+    mask = np.empty(n, np.uint8)
+    off = ctypes.c_int64(0)
+    P = (I32P * len(caps))(*[_p(c, I32P) for c in caps])
+    _check(_lib().jfc_load_mfi(_b(path), _p(e, I32P), P, ctypes.byref(off), _p(mask, U8P)), "jfc_load_mfi")
+    return info, e.reshape(shape), [c.reshape(shape) for c in caps], off.value, mask.reshape(shape)
+
+
+def save_mfi(path, excess, caps, maxflow, mask=None):
+    dims, w, h, d = _dims(np.shape(excess))
+    e = np.ascontiguousarray(excess, np.int32).ravel()
+    cs = [np.ascontiguousarray(c, np.int32).ravel() for c in caps]
+    m = None if mask is None else np.ascontiguousarray(mask, np.uint8).ravel()
+    P = (I32P * len(cs))(*[_p(c, I32P) for c in cs])
+    _check(_lib().jfc_save_mfi(_b(path), dims, w, h, d, _p(e, I32P), P, int(maxflow),
+                               None if m is None else _p(m, U8P)), "jfc_save_mfi")
 
 
 def graph_bytes(shape):

@@ -302,6 +302,69 @@ def test_batch_autotune_restores_and_matches(ctx):
     b.close()
 
 
+def test_solve_from_data_files(ctx, tmp_path):
+    """Graphs loaded from the reference's file formats solve to the recorded
+    max-flow: .ef/.c1/.c2 (flower, published value) and .mfi (its header)."""
+    shape, e, caps, published, ref_object = load_fixture("flower")
+    base = str(tmp_path / "flower")
+    jfcut.save_graph_files(base, e.reshape(shape), [c.reshape(shape) for c in caps])
+    g = jfcut.Graph(ctx, shape)
+    g.load_files(base)
+    g.solve()
+    assert g.flow() == published
+    jfcut.write_cut(base + ".cut", None, g.labels())
+    _, lab = jfcut.read_cut(base + ".cut", shape)
+    assert np.array_equal(lab, g.labels())
+    jfcut.save_mfi(base + ".mfi", e.reshape(shape), [c.reshape(shape) for c in caps], published)
+    g2 = jfcut.Graph(ctx, shape)
+    assert g2.load_mfi(base + ".mfi") == published
+    g2.solve()
+    assert g2.flow() == published
+    # a 3D instance with terminal caps on both sides of many nodes
+    rng = np.random.default_rng(31)
+    shp = (9, 20, 33)
+    e3, c3 = random_grid(shp, rng, cap_max=200)
+    f3, _, _, lab3 = oracle.maxflow(shp, e3, c3)
+    jfcut.save_mfi(base + "3.mfi", e3.reshape(shp), [c.reshape(shp) for c in c3], f3)
+    g3 = jfcut.Graph(ctx, shp)
+    assert g3.load_mfi(base + "3.mfi") == f3
+    g3.solve()
+    assert g3.flow() == f3 and np.array_equal(g3.labels().ravel(), lab3)
+    for x in (g, g2, g3):
+        x.close()
+
+
+def test_energy_certificate(ctx):
+    """data + smooth energy of the canonical cut over the original graph equals
+    the max-flow (device energy kernel vs oracle), 2D fixture and 3D random."""
+    import torch
+    cases = [load_fixture("sponge")[:4]]
+    rng = np.random.default_rng(41)
+    shp = (7, 19, 26)
+    e3, c3 = random_grid(shp, rng)
+    cases.append((shp, e3, c3, None))
+    for shape, e, caps, published in cases:
+        g, st = solve_set(ctx, shape, e, caps)
+        flow = g.flow()
+        if published is not None:
+            assert flow == published
+        lab = torch.from_numpy(g.labels().ravel().copy()).cuda()
+        de = torch.from_numpy(np.ascontiguousarray(e, np.int32).ravel()).cuda()
+        dc = [torch.from_numpy(np.ascontiguousarray(c, np.int32).ravel()).cuda() for c in caps]
+        torch.cuda.synchronize()
+        data, smooth = jfcut.energy_device(0, shape, de.data_ptr(), [c.data_ptr() for c in dc], lab.data_ptr())
+        assert data + smooth == flow
+        assert data + smooth == oracle.cut_energy(shape, e, caps, g.labels().ravel())
+        # a worse labelling has a higher energy
+        lab2 = lab.clone()
+        lab2[: lab2.numel() // 3] = 1 - lab2[: lab2.numel() // 3]
+        torch.cuda.synchronize()
+        d2, s2 = jfcut.energy_device(0, shape, de.data_ptr(), [c.data_ptr() for c in dc], lab2.data_ptr())
+        assert d2 + s2 >= flow
+        assert d2 + s2 == oracle.cut_energy(shape, e, caps, lab2.cpu().numpy())
+        g.close()
+
+
 def test_errors(ctx):
     img, seeds = jfcut.synth_gray_ellipse(64, 64, seed=1)
     g = jfcut.Graph(ctx, img.shape)

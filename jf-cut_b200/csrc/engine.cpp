@@ -218,6 +218,13 @@ static size_t pin_need(const TileSet& ts) {
   return sizeof(DevCounters) + sizeof(long long) * 2 * (size_t)ts.ngrids + 64;
 }
 
+// pinned slot holding the sweep pairs of the next push-relabel phase (after
+// the read-back area); copied to the control block by the cycle itself
+static int* pin_sweeps(jfc_ctx* ctx, const TileSet& ts) {
+  return (int*)((char*)ctx->h_pin + (pin_need(ts) + 255) / 256 * 256);
+}
+static size_t pin_need_cycle(const TileSet& ts) { return (pin_need(ts) + 255) / 256 * 256 + 64; }
+
 // Enqueue one BFS (global relabel when !cut, cut otherwise) and the read-back
 // of its counters (+ per-grid active tiles) into pinned memory `pin`.
 static cudaError_t enqueue_bfs(TileSet& ts, bool cut, int max_passes, cudaStream_t s, void* pin) {
@@ -279,7 +286,7 @@ int engine_bfs(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, bool cut, int& pa
 namespace {
 struct CycleGraphs {
   struct Entry {
-    int interval, local_iters, max_passes;
+    int local_iters, max_passes;
     void* pin;
     cudaGraphExec_t exec;
   };
@@ -296,21 +303,22 @@ void tileset_drop_graphs(TileSet& ts) {
   ts.gcache = nullptr;
 }
 
-static cudaError_t enqueue_cycle(TileSet& ts, int interval, int local_iters, int max_passes, cudaStream_t s,
+static cudaError_t enqueue_cycle(TileSet& ts, const int* pin_sw, int local_iters, int max_passes, cudaStream_t s,
                                  void* pin) {
   cudaError_t e = cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s);
-  if (e == cudaSuccess) e = launch_pr_phase(ts, interval, local_iters, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&ts.d_ctr->pr_sweeps, pin_sw, sizeof(int), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = launch_pr_phase(ts, 0, local_iters, s);
   if (e == cudaSuccess) e = enqueue_bfs(ts, false, max_passes, s, pin);
   return e;
 }
 
-static cudaGraphExec_t cycle_graph(TileSet& ts, int interval, int local_iters, int max_passes, cudaStream_t s,
+static cudaGraphExec_t cycle_graph(TileSet& ts, const int* pin_sw, int local_iters, int max_passes, cudaStream_t s,
                                    void* pin) {
   if (!ts.gcache) ts.gcache = new CycleGraphs();
   CycleGraphs* c = (CycleGraphs*)ts.gcache;
   if (c->broken) return nullptr;
   for (auto& e : c->v)
-    if (e.interval == interval && e.local_iters == local_iters && e.max_passes == max_passes && e.pin == pin)
+    if (e.local_iters == local_iters && e.max_passes == max_passes && e.pin == pin)
       return e.exec;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
@@ -323,7 +331,7 @@ static cudaGraphExec_t cycle_graph(TileSet& ts, int interval, int local_iters, i
     return nullptr;
   }
   g_capturing = true;
-  const cudaError_t e1 = enqueue_cycle(ts, interval, local_iters, max_passes, s, pin);
+  const cudaError_t e1 = enqueue_cycle(ts, pin_sw, local_iters, max_passes, s, pin);
   g_capturing = false;
   cudaGraph_t g = nullptr;
   const cudaError_t e2 = cudaStreamEndCapture(s, &g);
@@ -337,7 +345,7 @@ static cudaGraphExec_t cycle_graph(TileSet& ts, int interval, int local_iters, i
     c->broken = true;
     return nullptr;
   }
-  c->v.push_back({interval, local_iters, max_passes, pin, x});
+  c->v.push_back({local_iters, max_passes, pin, x});
   return x;
 }
 
@@ -346,16 +354,18 @@ static cudaGraphExec_t cycle_graph(TileSet& ts, int interval, int local_iters, i
 static int run_cycle(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, int interval, int& passes,
                      std::vector<int>& active, int* sweeps_done, bool* used_graph) {
   cudaStream_t s = ctx->stream;
-  int rc = pin_reserve(ctx, pin_need(ts));
+  int rc = pin_reserve(ctx, pin_need_cycle(ts));
   if (rc) return rc;
-  cudaGraphExec_t x = p.use_graph ? cycle_graph(ts, interval, p.local_iters, p.max_bfs_passes, s, ctx->h_pin)
+  int* pin_sw = pin_sweeps(ctx, ts);
+  *pin_sw = interval;   // the previous cycle's copies finished at its sync
+  cudaGraphExec_t x = p.use_graph ? cycle_graph(ts, pin_sw, p.local_iters, p.max_bfs_passes, s, ctx->h_pin)
                                   : nullptr;
   if (x) {
     JFC_CUDA(cudaGraphLaunch(x, s));
     jfc_note_launch(2);
     if (used_graph) *used_graph = true;
   } else {
-    JFC_CUDA(enqueue_cycle(ts, interval, p.local_iters, p.max_bfs_passes, s, ctx->h_pin));
+    JFC_CUDA(enqueue_cycle(ts, pin_sw, p.local_iters, p.max_bfs_passes, s, ctx->h_pin));
   }
   JFC_CUDA(cudaStreamSynchronize(s));
   return finish_bfs(ts, false, ctx->h_pin, passes, &active, nullptr, sweeps_done);
@@ -415,8 +425,17 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   // global relabels pay off; once only a sliver is active (long transport
   // paths, few tiles), the dense relabel dominates, so the interval doubles
   // (the push-relabel phase still stops as soon as its queues drain).
+  //  The interval also doubles while the last relabel cost more than twice
+  // the push-relabel phase before it (device clocks) and that phase used all
+  // its sweeps: the relabel is then the bottleneck and is amortised.
   int interval = p.relabel_interval;
   bool graphs = false;
+  unsigned long long last_pr = 0, last_gr = 0;
+  {
+    const DevCounters* c0 = (const DevCounters*)ctx->h_pin;
+    last_pr = c0->ns_pr;
+    last_gr = c0->ns_gr_first + c0->ns_gr_frontier;
+  }
   while (total() > 0) {
     if (st.sweeps >= p.max_sweeps) {
       status = set_error(JFC_ERR_NOT_CONVERGED, "sweep budget exhausted");
@@ -428,8 +447,16 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
     rc = run_cycle(ctx, ts, p, interval, st.bfs_passes, active, &sw, &graphs);
     if (rc) return rc;
     st.sweeps += sw;
-    if (total() * 256 < (long long)ts.ntiles) interval = std::min(interval * 2, p.relabel_interval_max);
-    else interval = p.relabel_interval;
+    {
+      const DevCounters* c1 = (const DevCounters*)ctx->h_pin;
+      const unsigned long long pr = c1->ns_pr - last_pr, gr = c1->ns_gr_first + c1->ns_gr_frontier - last_gr;
+      last_pr = c1->ns_pr;
+      last_gr = c1->ns_gr_first + c1->ns_gr_frontier;
+      const bool sliver = total() * 256 < (long long)ts.ntiles;
+      const bool relabel_bound = gr > 2 * pr && sw >= 2 * interval;
+      if (sliver || relabel_bound) interval = std::min(interval * 2, p.relabel_interval_max);
+      else interval = p.relabel_interval;
+    }
     ++st.global_relabels;
     if (p.verbose) {
       hc = (const DevCounters*)ctx->h_pin;

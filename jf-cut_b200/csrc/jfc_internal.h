@@ -50,7 +50,7 @@ struct DevCounters {
   int bfs_passes;            // passes of the last BFS
   int bfs_status;            // 1 converged, 2 pass budget exhausted
   int sweeps_done;           // sweeps run by the last push-relabel phase
-  int pad_;
+  int pr_sweeps;             // sweep pairs of the next phase when launched with sweeps <= 0
   unsigned long long visits; // push-relabel tile visits
   unsigned long long bfs_visits;
   unsigned long long rounds; // push/relabel rounds summed over visits
@@ -97,7 +97,9 @@ void jfc_note_launch(int n = 1);
 
 // ----------------------------------------------------------- kernel launchers
 // (kernels_pr.cu) `sweeps` parity sweeps (even tiles, then odd tiles, ...)
-// in one persistent launch, draining the device work queues
+// in one persistent launch, draining the device work queues; sweeps <= 0
+// reads the count from the control block (pr_sweeps), so one captured graph
+// serves every interval
 cudaError_t launch_pr_phase(const TileSet& ts, int sweeps, int local_iters, cudaStream_t s);
 // (kernels_bfs.cu) one BFS to its fixpoint in one persistent launch:
 // global relabel (cut = false; also refills the push-relabel queues) or the

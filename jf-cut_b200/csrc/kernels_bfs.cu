@@ -543,7 +543,7 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
 // BFS from the deficits, fused initialisation).  A plain launch: its many
 // registers do not limit the occupancy of the frontier kernel.
 template <int DIMS, int TY, int TZ>
-__global__ void __launch_bounds__(256, 2) k_relabel_first(TileSet ts) {
+__global__ void __launch_bounds__(256, (DIMS == 3 && TY * TZ > 8) ? 1 : 2) k_relabel_first(TileSet ts) {
   DevCounters* ctr = ts.d_ctr;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctr->t_gr_start = jfc::global_ns();
   const int lane = threadIdx.x & 31;

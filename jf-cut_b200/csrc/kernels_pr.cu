@@ -281,7 +281,8 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
   unsigned long long visits = 0, rounds = 0;
   const unsigned long long t0 = jfc::global_ns();
   int s = 0;
-  for (; s < 2 * sweeps; ++s) {
+  const int npairs = sweeps > 0 ? sweeps : jfc::vload(&ctr->pr_sweeps);
+  for (; s < 2 * npairs; ++s) {
     const int p = s & 1;
     const int b = jfc::vload(&ctr->cur_pr[p]);
     const int bo = jfc::vload(&ctr->cur_pr[p ^ 1]);

@@ -30,7 +30,8 @@ int rebuild(jfc_batch* b) {
   const int tr = b->ctx->params.tile_rows;
   for (int k = 0; k < 2; ++k) {
     const int dims = k ? 3 : 2;
-    const int code = shape_code(dims, tr);
+    const int td = b->ctx->params.tile_depth;
+    const int code = shape_code(dims, tr, td);
     if (!b->dirty && b->shape[k] == code) continue;
     std::vector<GridDev> v;
     for (jfc_graph* g : b->graphs)
@@ -38,7 +39,7 @@ int rebuild(jfc_batch* b) {
     tileset_free(b->ts[k]);
     b->shape[k] = -1;
     if (v.empty()) continue;
-    int rc = tileset_build(b->ts[k], dims, tr, v);
+    int rc = tileset_build(b->ts[k], dims, tr, td, v);
     if (rc) return rc;
     b->shape[k] = code;
   }

@@ -55,6 +55,8 @@ extern "C" const char* jfc_last_error(void) { return g_err.c_str(); }
 
 void fill_defaults(jfc_params& p) {
   if (p.tile_rows != 8 && p.tile_rows != 16) p.tile_rows = 16;
+  if (!(p.tile_depth == 1 || p.tile_depth == 2 || (p.tile_depth == 4 && p.tile_rows == 16)))
+    p.tile_depth = p.tile_rows == 16 ? 4 : 2;
   if (p.local_iters <= 0) p.local_iters = 16;
   if (p.relabel_interval <= 0) p.relabel_interval = 4;
   if (p.relabel_interval_max < p.relabel_interval) p.relabel_interval_max = 16 * p.relabel_interval;
@@ -68,7 +70,9 @@ double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
   return (double)ms;
 }
 
-int shape_code(int dims, int tile_rows) { return dims * 100 + tile_rows; }
+int shape_code(int dims, int tile_rows, int tile_depth) {
+  return dims * 1000 + tile_rows * 10 + (dims == 3 ? tile_depth : 0);
+}
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -115,12 +119,14 @@ static void tileset_carve(TileSet& ts, char* blk, size_t* total) {
   ts.d_ctr = (DevCounters*)(blk + o_ctr);
 }
 
-int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDev>& grids_in, cudaStream_t s) {
+int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const std::vector<GridDev>& grids_in,
+                  cudaStream_t s) {
   int TY, TZ;
   if (dims == 2) {
     TY = tile_rows; TZ = 1;
   } else {
-    TY = 4; TZ = tile_rows >= 16 ? 4 : 2;
+    TZ = tile_depth > 0 ? tile_depth : (tile_rows >= 16 ? 4 : 2);
+    TY = tile_rows / TZ;
   }
   std::vector<GridDev> grids = grids_in;
   int base = 0, npar[2] = {0, 0};

@@ -68,12 +68,12 @@ int engine_cut(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, std::vector<GridR
 // block is reused while it is large enough.  With a stream the grid and tile
 // tables are uploaded asynchronously from pinned staging (rewrite it only
 // after the next host sync on that stream) and a new block gets headroom.
-int tileset_build(TileSet& ts, int dims, int tile_rows, const std::vector<GridDev>& grids,
+int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const std::vector<GridDev>& grids,
                   cudaStream_t s = nullptr);
 void tileset_free(TileSet& ts);
 // Drop the tile set's captured relabel-cycle graphs.
 void tileset_drop_graphs(TileSet& ts);
-int shape_code(int dims, int tile_rows);
+int shape_code(int dims, int tile_rows, int tile_depth);
 
 int set_error(int code, const std::string& msg);
 int cuda_status(cudaError_t e, const char* where);

@@ -20,7 +20,8 @@
 #define JFC_INF (1 << 30)
 #define JFC_TW 32           // tile width = warp width
 #define JFC_PAD_Y2 16       // 2D row padding (covers tile heights 4, 8, 16)
-#define JFC_PAD_YZ3 4       // 3D y/z padding (covers 4x4, 4x2, 2x4 tiles)
+#define JFC_PAD_Y3 16       // 3D y padding (tile heights 4, 8, 16)
+#define JFC_PAD_Z3 4        // 3D z padding (tile depths 1, 2, 4)
 #define JFC_MAX_K 32        // k-means clusters per class
 #define JFC_TQ 65536        // t-link probability quantisation
 

@@ -539,6 +539,153 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
   flag_neighbours<DIMS, TY, TZ>(g, a, tid, rows_fin, c0 != 0, c31 != 0, false, Q);
 }
 
+// Frontier visit, one warp per tile: a level BFS over the tile (bit-parallel
+// rows as in the first pass) seeded by the halo heights, keeping only strict
+// improvements (heights only fall during a relabel, and a node is assigned
+// at the first level that reaches it).  Levels with an empty frontier jump
+// to the next halo seed that could improve its node, so a visit costs one
+// level per improved BFS layer plus one per distinct useful seed value:
+// bounded by the tile's nodes plus its halo cells.
+template <int DIMS, int TY, int TZ>
+__device__ __forceinline__ void relabel_frontier_warp(const TileSet& ts, int tid, const BfsQ& Q, int& cur_grid,
+                                                      int& delta) {
+  constexpr int R = TY * TZ;
+  constexpr int kMaxLevels = 4096;   // above the bound (nodes + halo cells); never reached
+  const int lane = threadIdx.x & 31;
+  const int4 ti = ts.d_info[tid];
+  const GridDev& g = ts.d_desc[ti.x];
+  const Addr a = make_addr<DIMS, TY, TZ>(g, ti, lane);
+  unsigned AXP[R], AXM[R], AYP[R], AYM[R];
+  unsigned AZP[DIMS == 3 ? R : 1], AZM[DIMS == 3 ? R : 1];
+  int hv[R];
+  unsigned posm = 0;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const long long n = roff<TY>(a, i);
+    const unsigned b = g.label[n];   // arc byte written by the first pass
+    hv[i] = g.h[n];
+    AXP[i] = __ballot_sync(FULL, b & jfc::A_XP);
+    AXM[i] = __ballot_sync(FULL, b & jfc::A_XM);
+    AYP[i] = __ballot_sync(FULL, b & jfc::A_YP);
+    AYM[i] = __ballot_sync(FULL, b & jfc::A_YM);
+    if constexpr (DIMS == 3) {
+      AZP[i] = __ballot_sync(FULL, b & jfc::A_ZP);
+      AZM[i] = __ballot_sync(FULL, b & jfc::A_ZM);
+    }
+    if (b & 128u) posm |= 1u << i;
+  }
+  // halo heights: y faces per z slice (lane = x), z faces per row y, x faces
+  // in lanes r (left of row r) and 16 + r (right of row r)
+  int HT[TZ], HB[TZ];
+#pragma unroll
+  for (int z = 0; z < TZ; ++z) {
+    const long long n = roff<TY>(a, z * TY);
+    HT[z] = a.has_yT ? g.h[n - a.pitch] : JFC_INF;
+    HB[z] = a.has_yB ? g.h[n + (long long)TY * a.pitch] : JFC_INF;
+  }
+  int HZT[DIMS == 3 ? TY : 1], HZB[DIMS == 3 ? TY : 1];
+  if constexpr (DIMS == 3) {
+#pragma unroll
+    for (int y = 0; y < TY; ++y) {
+      const long long n = roff<TY>(a, y);
+      HZT[y] = a.has_zT ? g.h[n - a.slab] : JFC_INF;
+      HZB[y] = a.has_zB ? g.h[n + (long long)TZ * a.slab] : JFC_INF;
+    }
+  }
+  int HX = JFC_INF;
+  const int xrow = lane & 15;
+  {
+    const bool left = lane < 16;
+    if (xrow < R && (left ? a.has_xL : a.has_xR))
+      HX = g.h[(long long)(left ? a.x0 - 1 : a.x0 + 32) + (long long)(a.y0 + xrow % TY) * a.pitch +
+               (long long)(a.z0 + xrow / TY) * a.slab];
+  }
+  // smallest seed level above d that could still improve its node
+  auto next_level = [&](int d) -> int {
+    int c = JFC_INF;
+#pragma unroll
+    for (int z = 0; z < TZ; ++z) {
+      const int it = z * TY, ib = z * TY + TY - 1;
+      int v = HT[z] + 1;
+      if (v > d && v < hv[it] && ((AYM[it] >> lane) & 1u)) c = min(c, v);
+      v = HB[z] + 1;
+      if (v > d && v < hv[ib] && ((AYP[ib] >> lane) & 1u)) c = min(c, v);
+    }
+    if constexpr (DIMS == 3) {
+#pragma unroll
+      for (int y = 0; y < TY; ++y) {
+        const int it = y, ib = (TZ - 1) * TY + y;
+        int v = HZT[y] + 1;
+        if (v > d && v < hv[it] && ((AZM[it] >> lane) & 1u)) c = min(c, v);
+        v = HZB[y] + 1;
+        if (v > d && v < hv[ib] && ((AZP[ib] >> lane) & 1u)) c = min(c, v);
+      }
+    }
+    if (xrow < R && HX + 1 > d) c = min(c, HX + 1);
+    return __reduce_min_sync(FULL, c);
+  };
+  unsigned F[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) F[i] = 0u;
+  unsigned rows_changed = 0, c0 = 0, c31 = 0;
+  bool again = false;
+  int d = next_level(-1);
+  for (int level = 0; d < JFC_INF; ++level) {
+    if (level >= kMaxLevels) { again = true; break; }
+    const unsigned sx = __ballot_sync(FULL, HX + 1 == d);
+    unsigned N[R];
+    unsigned any = 0;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int y = i % TY, z = i / TY;
+      unsigned m = ((F[i] >> 1) & AXP[i]) | ((F[i] << 1) & AXM[i]);
+      if (y < TY - 1) m |= F[(i + 1 < R) ? i + 1 : i] & AYP[i];
+      if (y > 0) m |= F[(i > 0) ? i - 1 : 0] & AYM[i];
+      if constexpr (DIMS == 3) {
+        if (z < TZ - 1) m |= F[(i + TY < R) ? i + TY : i] & AZP[i];
+        if (z > 0) m |= F[(i >= TY) ? i - TY : 0] & AZM[i];
+        if (z == 0) m |= __ballot_sync(FULL, HZT[y] + 1 == d) & AZM[i];
+        if (z == TZ - 1) m |= __ballot_sync(FULL, HZB[y] + 1 == d) & AZP[i];
+      }
+      if (y == 0) m |= __ballot_sync(FULL, HT[z] + 1 == d) & AYM[i];
+      if (y == TY - 1) m |= __ballot_sync(FULL, HB[z] + 1 == d) & AYP[i];
+      m |= ((sx >> i) & 1u) & AXM[i];
+      m |= (((sx >> (16 + i)) & 1u) << 31) & AXP[i];
+      N[i] = m & __ballot_sync(FULL, hv[i] > d);
+      any |= N[i];
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      F[i] = N[i];
+      if (N[i]) {
+        rows_changed |= 1u << i;
+        c0 |= N[i] & 1u;
+        c31 |= N[i] >> 31;
+        if ((N[i] >> lane) & 1u) {
+          hv[i] = d;
+          g.h[roff<TY>(a, i)] = d;
+        }
+      }
+    }
+    d = any ? d + 1 : next_level(d);
+  }
+  bool act = false;
+#pragma unroll
+  for (int i = 0; i < R; ++i) act |= ((posm >> i) & 1u) && hv[i] < JFC_INF;
+  act = __any_sync(FULL, act);
+  if (lane == 0) {
+    const int old = (int)ts.d_act[tid];
+    ts.d_act[tid] = act ? 1 : 0;
+    if (ti.x != cur_grid) {
+      if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
+      delta = 0;
+      cur_grid = ti.x;
+    }
+    delta += (act ? 1 : 0) - old;
+  }
+  flag_neighbours<DIMS, TY, TZ>(g, a, tid, rows_changed, c0 != 0, c31 != 0, again, Q);
+}
+
 // Global relabel, pass 0: every tile, one warp per tile (bit-parallel level
 // BFS from the deficits, fused initialisation).  A plain launch: its many
 // registers do not limit the occupancy of the frontier kernel.
@@ -560,8 +707,93 @@ __global__ void __launch_bounds__(256, (DIMS == 3 && TY * TZ > 8) ? 1 : 2) k_rel
 // the push-relabel queues are refilled with every tile holding an active node
 // (the reference's graphcut_count_node + clogs scan + graphcut_scatter_node,
 // graphcut_count_block.cl:19-65, as one warp-aggregated append).
+// Warp form of the frontier passes: one warp per queued tile (3D: many
+// tiles per pass, so the visit throughput counts).
 template <int DIMS, int TY, int TZ>
-__global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel(TileSet ts, int max_passes) {
+__global__ void __launch_bounds__(256) k_relabel_warp(TileSet ts, int max_passes) {
+  DevCounters* ctr = ts.d_ctr;
+  const int lane = threadIdx.x & 31;
+  unsigned long long visits = 0;
+  int cur_grid = -1, delta = 0;
+  bool ok = true;
+  int pass = 1;
+  const unsigned long long t1 = jfc::global_ns();
+  for (pass = 1; ok; ++pass) {
+    const int cb = pass & 1;
+    const int n = jfc::vload(&ctr->qn_bfs[cb]);
+    if (n == 0) break;
+    if (pass > max_passes) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) ctr->bfs_status = 2;
+      break;
+    }
+    BfsQ Q{ts.d_flag_bfs[cb ^ 1], ts.d_q_bfs[cb ^ 1], &ctr->qn_bfs[cb ^ 1]};
+    const int* queue = ts.d_q_bfs[cb];
+    int* fcur = ts.d_flag_bfs[cb];
+    for (;;) {
+      const unsigned k = jfc::warp_ticket(&ctr->ticket[cb]);
+      if ((int)k >= n) break;
+      const int tt = queue[k];
+      if (lane == 0) fcur[tt] = 0;
+      __syncwarp();
+      relabel_frontier_warp<DIMS, TY, TZ>(ts, tt, Q, cur_grid, delta);
+      ++visits;
+    }
+    ok = jfc::grid_sync(ctr, [&]() {
+      ctr->ticket[cb] = 0;
+      ctr->qn_bfs[cb] = 0;
+    });
+  }
+  if (lane == 0 && delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
+  // refill the push-relabel queues (buffer 0 of each parity) from the
+  // active-tile flags
+  if (ok) ok = jfc::grid_sync(ctr, [&]() {
+    ctr->qn_pr[0][0] = ctr->qn_pr[0][1] = ctr->qn_pr[1][0] = ctr->qn_pr[1][1] = 0;
+    ctr->cur_pr[0] = ctr->cur_pr[1] = 0;
+  });
+  if (ok) {
+    for (;;) {
+      const unsigned c = jfc::warp_ticket(&ctr->ticket[0]);
+      const long long b = (long long)c * 32;
+      if (b >= ts.ntiles) break;
+      const long long t = b + lane;
+      bool act = false;
+      int par = 0;
+      if (t < ts.ntiles) {
+        act = ts.d_act[t] != 0;
+        ts.d_flag_pr[t] = act ? 1 : 0;
+        if (act) { const int4 ti = ts.d_info[t]; par = (ti.y + ti.z + ti.w) & 1; }
+      }
+      jfc::warp_append(act && par == 0, (int)t, nullptr, ts.d_q_pr[0][0], &ctr->qn_pr[0][0]);
+      jfc::warp_append(act && par == 1, (int)t, nullptr, ts.d_q_pr[1][0], &ctr->qn_pr[1][0]);
+    }
+    ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
+  }
+  // frontier visits are counted per warp (lane 0); pass 0 visited every tile
+  __shared__ unsigned long long s_vis;
+  if (threadIdx.x == 0) s_vis = 0;
+  __syncthreads();
+  if (lane == 0 && visits) atomicAdd(&s_vis, visits);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_vis) atomicAdd(&ctr->bfs_visits, s_vis);
+    if (blockIdx.x == 0) {
+      ctr->bfs_passes = pass;
+      ctr->bfs_visits += (unsigned long long)ts.ntiles;
+      if (ctr->bfs_status == 0) ctr->bfs_status = 1;
+      const unsigned long long t2 = jfc::global_ns();
+      ctr->ns_gr_first += t1 - ctr->t_gr_start;
+      ctr->ns_gr_frontier += t2 - t1;
+    }
+  }
+}
+
+// Global relabel, frontier passes (persistent, cooperative), CTA form: one
+// CTA per queued tile (2D: few tiles per pass, so the visit latency counts), grid barrier between passes, until a pass queues nothing; then
+// the push-relabel queues are refilled with every tile holding an active node
+// (the reference's graphcut_count_node + clogs scan + graphcut_scatter_node,
+// graphcut_count_block.cl:19-65, as one warp-aggregated append).
+template <int DIMS, int TY, int TZ>
+__global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet ts, int max_passes) {
   __shared__ RlSmem<DIMS, TY, TZ> sm;
   DevCounters* ctr = ts.d_ctr;
   const int lane = threadIdx.x & 31;
@@ -685,8 +917,12 @@ __global__ void __launch_bounds__(256) k_grid_sums(const GridDev* __restrict__ g
 
 template <int DIMS, int TY, int TZ, bool CUT>
 cudaError_t bfs_t(const TileSet& ts, int max_passes, cudaStream_t s) {
-  const void* fn = CUT ? (const void*)k_cut<DIMS, TY, TZ> : (const void*)k_relabel<DIMS, TY, TZ>;
-  const int nt = CUT ? 256 : RTile<DIMS, TY, TZ>::NT;
+  // global relabel frontier passes: CTA per tile in 2D, warp per tile in 3D
+  const void* fn;
+  if constexpr (CUT) fn = (const void*)k_cut<DIMS, TY, TZ>;
+  else if constexpr (DIMS == 2) fn = (const void*)k_relabel_cta<DIMS, TY, TZ>;
+  else fn = (const void*)k_relabel_warp<DIMS, TY, TZ>;
+  const int nt = (CUT || DIMS == 3) ? 256 : RTile<DIMS, TY, TZ>::NT;
   static int blocks = 0;
   if (!blocks) blocks = persistent_blocks(fn, nt, 0);
   if (!CUT) {
@@ -803,6 +1039,9 @@ cudaError_t launch_bfs(const TileSet& ts, bool cut, int max_passes, cudaStream_t
   }
   if (ts.TY == 4 && ts.TZ == 4) return JFC_BFS(3, 4, 4);
   if (ts.TY == 4 && ts.TZ == 2) return JFC_BFS(3, 4, 2);
+  if (ts.TY == 16 && ts.TZ == 1) return JFC_BFS(3, 16, 1);
+  if (ts.TY == 8 && ts.TZ == 2) return JFC_BFS(3, 8, 2);
+  if (ts.TY == 8 && ts.TZ == 1) return JFC_BFS(3, 8, 1);
 #undef JFC_BFS
   return cudaErrorInvalidValue;
 }
@@ -817,6 +1056,9 @@ cudaError_t launch_grid_sums(const TileSet& ts, cudaStream_t s) {
   }
   if (ts.TY == 4 && ts.TZ == 4) return sums_t<4, 4>(ts, s);
   if (ts.TY == 4 && ts.TZ == 2) return sums_t<4, 2>(ts, s);
+  if (ts.TY == 16 && ts.TZ == 1) return sums_t<16, 1>(ts, s);
+  if (ts.TY == 8 && ts.TZ == 2) return sums_t<8, 2>(ts, s);
+  if (ts.TY == 8 && ts.TZ == 1) return sums_t<8, 1>(ts, s);
   return cudaErrorInvalidValue;
 }
 

@@ -347,5 +347,8 @@ cudaError_t launch_pr_phase(const TileSet& ts, int sweeps, int local_iters, cuda
   }
   if (ts.TY == 4 && ts.TZ == 4) return launch_t<3, 4, 4>(ts, sweeps, local_iters, s);
   if (ts.TY == 4 && ts.TZ == 2) return launch_t<3, 4, 2>(ts, sweeps, local_iters, s);
+  if (ts.TY == 16 && ts.TZ == 1) return launch_t<3, 16, 1>(ts, sweeps, local_iters, s);
+  if (ts.TY == 8 && ts.TZ == 2) return launch_t<3, 8, 2>(ts, sweeps, local_iters, s);
+  if (ts.TY == 8 && ts.TZ == 1) return launch_t<3, 8, 1>(ts, sweeps, local_iters, s);
   return cudaErrorInvalidValue;
 }

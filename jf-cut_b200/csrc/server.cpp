@@ -325,7 +325,7 @@ void solver_loop(jfc_server* S) {
       if (changed[k]) {
         std::vector<GridDev> grids;
         for (Member& m : mem[k]) grids.push_back(m.s->G->g);
-        int rc = tileset_build(S->ts[k], k ? 3 : 2, p.tile_rows, grids, ctx->stream);
+        int rc = tileset_build(S->ts[k], k ? 3 : 2, p.tile_rows, p.tile_depth, grids, ctx->stream);
         if (rc) { fail_all(rc); return; }
       }
       int passes = 0, sw = 0;
@@ -346,7 +346,7 @@ void solver_loop(jfc_server* S) {
       if (conv.empty()) continue;
       std::vector<GridDev> grids;
       for (size_t i : conv) grids.push_back(mem[k][i].s->G->g);
-      int rc = tileset_build(S->cut_ts[k], k ? 3 : 2, p.tile_rows, grids, ctx->stream);
+      int rc = tileset_build(S->cut_ts[k], k ? 3 : 2, p.tile_rows, p.tile_depth, grids, ctx->stream);
       if (rc) { fail_all(rc); return; }
       std::vector<GridResult> res;
       int passes = 0;

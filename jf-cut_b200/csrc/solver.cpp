@@ -24,8 +24,8 @@ void grid_layout(int dims, int w, int h, int d, int& pitch, int& Hp, int& Dp) {
     Hp = (h + JFC_PAD_Y2 - 1) / JFC_PAD_Y2 * JFC_PAD_Y2;
     Dp = 1;
   } else {
-    Hp = (h + JFC_PAD_YZ3 - 1) / JFC_PAD_YZ3 * JFC_PAD_YZ3;
-    Dp = (d + JFC_PAD_YZ3 - 1) / JFC_PAD_YZ3 * JFC_PAD_YZ3;
+    Hp = (h + JFC_PAD_Y3 - 1) / JFC_PAD_Y3 * JFC_PAD_Y3;
+    Dp = (d + JFC_PAD_Z3 - 1) / JFC_PAD_Z3 * JFC_PAD_Z3;
   }
 }
 
@@ -61,10 +61,10 @@ cudaError_t copy_plane(void* padded, const void* dense, size_t elem, const jfc_g
 }
 
 int ensure_tileset(jfc_graph* G) {
-  const int code = shape_code(G->dims, G->ctx->params.tile_rows);
+  const int code = shape_code(G->dims, G->ctx->params.tile_rows, G->ctx->params.tile_depth);
   if (G->ts_shape == code) return JFC_OK;
   std::vector<GridDev> v{G->g};
-  int rc = tileset_build(G->ts, G->dims, G->ctx->params.tile_rows, v);
+  int rc = tileset_build(G->ts, G->dims, G->ctx->params.tile_rows, G->ctx->params.tile_depth, v);
   if (rc) return rc;
   G->ts_shape = code;
   return JFC_OK;
@@ -336,6 +336,9 @@ int jfc_set_params(jfc_ctx* c, const jfc_params* params) {
   if (!c || !params) return set_error(JFC_ERR_INVALID_ARG, "null argument");
   if (params->tile_rows && params->tile_rows != 8 && params->tile_rows != 16)
     return set_error(JFC_ERR_INVALID_ARG, "tile_rows must be 8 or 16");
+  // tile depth 4 with tile_rows 8 falls back to the default depth (2)
+  if (params->tile_depth && params->tile_depth != 1 && params->tile_depth != 2 && params->tile_depth != 4)
+    return set_error(JFC_ERR_INVALID_ARG, "tile_depth must be 1, 2 or 4");
   c->params = *params;
   fill_defaults(c->params);
   return JFC_OK;

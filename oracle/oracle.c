@@ -287,6 +287,17 @@ static void global_relabel(const grid_t* g, const int64_t* e, int32_t* const* r,
   }
 }
 
+void orc_sink_distances(int dims, int w, int h, int d, const int32_t* e32, const int32_t* const* r,
+                        int32_t* dist) {
+  grid_t g; grid_init(&g, dims, w, h, d);
+  int64_t* e = (int64_t*)malloc(sizeof(int64_t) * g.n);
+  int64_t* queue = (int64_t*)malloc(sizeof(int64_t) * (g.n + 1));
+  for (int64_t i = 0; i < g.n; ++i) e[i] = e32[i];
+  global_relabel(&g, e, (int32_t* const*)r, dist, queue);
+  free(e);
+  free(queue);
+}
+
 int64_t orc_maxflow(int dims, int w, int h, int d, int32_t* e32, int32_t* const* r,
                     uint8_t* labels) {
   grid_t g; grid_init(&g, dims, w, h, d);

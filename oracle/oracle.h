@@ -44,6 +44,12 @@ void orc_contrast_sum(int dims, int w, int h, int d, int pixfmt, const void* img
 int64_t orc_maxflow(int dims, int w, int h, int d, int32_t* e, int32_t* const* caps,
                     uint8_t* labels);
 
+/* Exact BFS distance of every node to the nearest deficit (e < 0) along
+ * residual arcs (the global relabel, graphcut_global_relabel.cl:19-124);
+ * unreachable nodes get 0x3fffffff. */
+void orc_sink_distances(int dims, int w, int h, int d, const int32_t* e, const int32_t* const* r,
+                        int32_t* dist);
+
 /* Reachability from {e > 0} along residual arcs (graphcut_compute_cut.cl).
  * Returns the number of reached nodes with e < 0 (0 for a maximum preflow). */
 int64_t orc_cut_from_residual(int dims, int w, int h, int d, const int32_t* e,

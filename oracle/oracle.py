@@ -116,6 +116,19 @@ def cut_from_residual(shape, e, r):
     return lab, int(bad)
 
 
+ORC_INF = 0x3FFFFFFF
+
+
+def sink_distances(shape, e, r):
+    """Exact residual BFS distance to the nearest deficit (ORC_INF if none)."""
+    dims, w, h, d = _shape(shape)
+    e = np.ascontiguousarray(e, dtype=np.int32)
+    keep, P = _ptrs(r)
+    out = np.empty(e.size, np.int32)
+    lib().orc_sink_distances(dims, w, h, d, e.ctypes.data_as(I32P), P, out.ctypes.data_as(I32P))
+    return out
+
+
 def cut_energy(shape, e0, caps0, labels):
     dims, w, h, d = _shape(shape)
     e0 = np.ascontiguousarray(e0, dtype=np.int32)

@@ -98,6 +98,50 @@ def test_random_grids(ctx, shape, seed):
     check_against_oracle(shape, e, caps, g.flow(), g.labels(), offset=seed * 7)
 
 
+@pytest.mark.parametrize("tile_rows,tile_depth", [(16, 4), (16, 2), (16, 1), (8, 2), (8, 1)])
+def test_3d_tile_shapes(ctx, tile_rows, tile_depth):
+    """Every 3D tile shape (32 x rows/depth x depth) gives the oracle's flow and cut."""
+    base = ctx.params()
+    try:
+        ctx.set_params(tile_rows=tile_rows, tile_depth=tile_depth)
+        for k, shape in enumerate([(5, 5, 5), (3, 17, 9), (13, 40, 70), (20, 33, 18)]):
+            rng = np.random.default_rng(500 + k)
+            e, caps = random_grid(shape, rng, cap_max=60, density=0.4)
+            g, st = solve_set(ctx, shape, e, caps)
+            check_against_oracle(shape, e, caps, g.flow(), g.labels())
+            g.close()
+        img, seeds = jfcut.synth_rgb_video(80, 48, 6, seed=11)
+        g = jfcut.Graph(ctx, seeds.shape)
+        g.build_from_image(img, seeds, jfcut.PIX_RGB8, dict(MODEL5, z_weight_pct=50))
+        e0, c0, _ = g.state()
+        g.solve()
+        f, _, _, lab = oracle.maxflow(seeds.shape, e0, c0)
+        assert np.array_equal(g.labels().ravel(), lab)
+        g.close()
+    finally:
+        ctx.set_params(tile_rows=base.tile_rows, tile_depth=base.tile_depth)
+
+
+@pytest.mark.parametrize("shape,tile_rows,tile_depth", [((64, 96), 16, 4), ((33, 65), 8, 2), ((100, 1000), 16, 4),
+                                                      ((8, 33, 31), 16, 4), ((13, 40, 70), 8, 2), ((9, 21, 40), 16, 1)])
+def test_final_heights_are_exact_distances(ctx, shape, tile_rows, tile_depth):
+    """The last global relabel of a solve leaves the exact residual BFS
+    distance to the deficits in every node (INF where none is reachable)."""
+    base = ctx.params()
+    try:
+        ctx.set_params(tile_rows=tile_rows, tile_depth=tile_depth)
+        rng = np.random.default_rng(sum(shape))
+        e, caps = random_grid(shape, rng, cap_max=40, density=0.35)
+        g, st = solve_set(ctx, shape, e, caps)
+        ef, rf, hf = g.state()
+        dist = oracle.sink_distances(shape, ef, rf)
+        dist[dist == oracle.ORC_INF] = 1 << 30
+        assert np.array_equal(hf, dist)
+        g.close()
+    finally:
+        ctx.set_params(tile_rows=base.tile_rows, tile_depth=base.tile_depth)
+
+
 def test_long_paths(ctx):
     # a serpentine corridor: flow has to travel across many tiles
     h, w = 96, 200

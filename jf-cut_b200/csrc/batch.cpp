@@ -170,7 +170,8 @@ int jfc_batch_autotune(jfc_batch* b, jfc_params* chosen) {
     return r == JFC_ERR_NOT_CONVERGED ? JFC_OK : r;
   };
   // Coordinate descent from the context's schedule: relabel interval, then
-  // rounds per visit, then tile height; each axis keeps its best value.  The
+  // rounds per visit, then tile height (then 3D tile depth when the batch has
+  // volumes); each axis keeps its best value.  The
   // first trial also pays one-time costs (tile set, graph capture), so the
   // starting point is timed twice.
   jfc_params best = base;
@@ -182,13 +183,17 @@ int jfc_batch_autotune(jfc_batch* b, jfc_params* chosen) {
   const int intervals[] = {2, 4, 8, 16};
   const int iters[] = {8, 16, 32};
   const int rows[] = {8, 16};
-  for (int axis = 0; axis < 3; ++axis) {
-    const int* vals = axis == 0 ? intervals : axis == 1 ? iters : rows;
-    const int nv = axis == 0 ? 4 : axis == 1 ? 3 : 2;
+  const int depths[] = {0, 1, 2, 4};   // 3D tile depth (0 = automatic 32x4x2)
+  bool has3d = false;
+  for (jfc_graph* g : b->graphs) has3d |= g->dims == 3;
+  for (int axis = 0; axis < (has3d ? 4 : 3); ++axis) {
+    const int* vals = axis == 0 ? intervals : axis == 1 ? iters : axis == 2 ? rows : depths;
+    const int nv = axis == 0 ? 4 : axis == 1 ? 3 : axis == 2 ? 2 : 4;
     const jfc_params center = best;
     for (int i = 0; i < nv; ++i) {
       jfc_params p = center;
-      int& field = axis == 0 ? p.relabel_interval : axis == 1 ? p.local_iters : p.tile_rows;
+      if (axis == 3 && vals[i] == 4 && p.tile_rows != 16) continue;
+      int& field = axis == 0 ? p.relabel_interval : axis == 1 ? p.local_iters : axis == 2 ? p.tile_rows : p.tile_depth;
       if (field == vals[i]) continue;
       field = vals[i];
       rc = trial(p, ms);

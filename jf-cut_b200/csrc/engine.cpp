@@ -55,8 +55,9 @@ extern "C" const char* jfc_last_error(void) { return g_err.c_str(); }
 
 void fill_defaults(jfc_params& p) {
   if (p.tile_rows != 8 && p.tile_rows != 16) p.tile_rows = 16;
-  if (!(p.tile_depth == 1 || p.tile_depth == 2 || (p.tile_depth == 4 && p.tile_rows == 16)))
-    p.tile_depth = p.tile_rows == 16 ? 4 : 2;
+  // 3D tile depth: 0 = automatic (32 x 4 x 2 tiles); 4 needs tile_rows 16
+  if (p.tile_depth == 4 && p.tile_rows == 8) p.tile_depth = 2;
+  if (p.tile_depth != 1 && p.tile_depth != 2 && p.tile_depth != 4) p.tile_depth = 0;
   if (p.local_iters <= 0) p.local_iters = 16;
   if (p.relabel_interval <= 0) p.relabel_interval = 4;
   if (p.relabel_interval_max < p.relabel_interval) p.relabel_interval_max = 16 * p.relabel_interval;
@@ -125,8 +126,10 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const st
   if (dims == 2) {
     TY = tile_rows; TZ = 1;
   } else {
-    TZ = tile_depth > 0 ? tile_depth : (tile_rows >= 16 ? 4 : 2);
-    TY = tile_rows / TZ;
+    // automatic 3D shape: 32 x 4 x 2 (measured best on the video workload:
+    // small tiles in y and z keep the relabel and push waves moving)
+    TZ = tile_depth > 0 ? tile_depth : 2;
+    TY = tile_depth > 0 ? tile_rows / tile_depth : 4;
   }
   std::vector<GridDev> grids = grids_in;
   int base = 0, npar[2] = {0, 0};

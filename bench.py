@@ -163,6 +163,27 @@ def cpu_baseline_bk():
                       "workload x%d, init+maxflow+labels" % (shape[1], shape[0], reps)}
 
 
+def max_over_ranks(x, dist=None, device="cuda"):
+    """The slowest rank's value (timings are taken per rank on the device)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(nodes_per_rank, world, steps, ms_max):
+    """Whole-job Mnodes/s of N independent replicas: every rank solved
+    nodes_per_rank per step; the job takes the slowest rank's time."""
+    return world * nodes_per_rank * steps / (ms_max / 1000.0) / 1e6
+
+
+def replica_seed(rank):
+    """Each rank solves its own replica (same shape, its own seed)."""
+    return SEED + rank
+
+
 def pct(v, q):
     return float(np.percentile(np.asarray(v, dtype=np.float64), q)) if len(v) else None
 
@@ -443,7 +464,7 @@ def main():
 
     w, h = args.width, args.height
     n = w * h
-    img, seeds = make_workload(w, h, SEED + rank)
+    img, seeds = make_workload(w, h, replica_seed(rank))
     stream = torch.cuda.Stream()
     ctx = jfcut.Context(local)
     ctx.set_stream(stream.cuda_stream)
@@ -474,12 +495,6 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -508,7 +523,7 @@ def main():
         ms = ev0.elapsed_time(ev1)
         launches = jfcut.kernel_launches() - l0
         clk = clocks.stop()
-        ms = max_over_ranks(ms)
+        ms = max_over_ranks(ms, dist)
         # ---- e2e: host buffers through the C ABI
         for _ in range(1):
             step_e2e()
@@ -519,11 +534,11 @@ def main():
             assert g.flow() == flow_ref
         ev1.record(stream)
         barrier()
-        ms_e2e = max_over_ranks(ev0.elapsed_time(ev1))
+        ms_e2e = max_over_ranks(ev0.elapsed_time(ev1), dist)
 
     ms_step = ms / args.steps
-    value = world * n * args.steps / (ms / 1000.0) / 1e6
-    e2e = world * n * args.steps / (ms_e2e / 1000.0) / 1e6
+    value = replica_throughput(n, world, args.steps, ms)
+    e2e = replica_throughput(n, world, args.steps, ms_e2e)
     tr = ctx.params().tile_rows
     bytes_per_visit = 32 * tr * 48 + (2 * 32 + 2 * tr) * 12
     achieved = visits * bytes_per_visit / (ms_pr / 1000.0) / 1e9 if ms_pr > 0 else 0.0

@@ -260,6 +260,13 @@ typedef struct jfc_server_stats {
 } jfc_server_stats;
 int  jfc_server_get_stats(jfc_server* s, jfc_server_stats* out);
 
+/* Tag post-process of a solved graph (QGCWidget::computeTag,
+ * QGCWidget.cpp:3275-3308; graphcut_compute_tag.cl): tag[i] = 1 for object
+ * nodes connected through object nodes (4 / 6-neighbourhood) to a foreground
+ * seed, else 0.  seeds: host dense JFC_SEED_* array, or NULL for the seeds of
+ * the graph's image build. */
+int jfc_graph_compute_tag(jfc_graph* g, const uint8_t* seeds, uint8_t* tag);
+
 /* Energy of a labelling over a graph given as dense device arrays (the
  * reference's energy check after a solve, QGCWidget.cpp:2452-2520):
  * data = sum over background nodes of max(e, 0) + sum over object nodes of

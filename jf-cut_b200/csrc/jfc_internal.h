@@ -92,6 +92,8 @@ struct TileSet {
 // out[1] smooth (int64 sums, out zeroed by the caller)
 cudaError_t launch_energy(int dims, int w, int h, int d, const int32_t* e, const int32_t* const* caps,
                           const uint8_t* lab, unsigned long long* out, cudaStream_t s);
+// (kernels_post.cu) p[i] &= keep over n bytes
+cudaError_t launch_and_bytes(uint8_t* p, long long n, uint8_t keep, cudaStream_t s);
 
 // Counts every kernel launch of the library (engine.cpp).
 void jfc_note_launch(int n = 1);
@@ -106,6 +108,9 @@ cudaError_t launch_pr_phase(const TileSet& ts, int sweeps, int local_iters, cuda
 // global relabel (cut = false; also refills the push-relabel queues) or the
 // source-side cut (cut = true)
 cudaError_t launch_bfs(const TileSet& ts, bool cut, int max_passes, cudaStream_t s);
+// (kernels_bfs.cu) tag post-process: bit 1 of each label byte = object node
+// connected through object nodes to a foreground seed (dense d_seeds)
+cudaError_t launch_tag(const TileSet& ts, const uint8_t* d_seeds, int max_passes, cudaStream_t s);
 cudaError_t launch_grid_sums(const TileSet& ts, cudaStream_t s);
 cudaError_t launch_clear_counters(const TileSet& ts, cudaStream_t s);
 int persistent_blocks(const void* kernel, int threads, size_t smem);

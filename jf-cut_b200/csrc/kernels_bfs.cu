@@ -119,9 +119,13 @@ __device__ __forceinline__ unsigned close_left(unsigned p, unsigned m) {
   return p;
 }
 
-template <int DIMS, int TY, int TZ, bool FIRST>
+// TAG: the reference's tag post-process (graphcut_compute_tag.cl) on the same
+// machinery: reachability from the foreground seeds through object nodes
+// (any direction), kept in bit 1 of the label byte; `seeds` is the dense
+// seed array (JFC_SEED_FG = 1).
+template <int DIMS, int TY, int TZ, bool FIRST, bool TAG = false>
 __device__ __forceinline__ void cut_tile(const GridDev& g, int4 ti, int tid, const BfsQ& Q,
-                                         int* __restrict__ bad) {
+                                         int* __restrict__ bad, const uint8_t* __restrict__ seeds = nullptr) {
   using D = Dirs<DIMS>;
   constexpr int R = TY * TZ;
   const int lane = threadIdx.x & 31;
@@ -131,7 +135,38 @@ __device__ __forceinline__ void cut_tile(const GridDev& g, int4 ti, int tid, con
   unsigned L[R], L0[R], IXL[R], IXR[R], IYU[R], IYD[R];
   unsigned IZU[DIMS == 3 ? R : 1], IZD[DIMS == 3 ? R : 1];
   unsigned NEG[R];
-  {
+  // dense index of this lane's node in row i (seed lookup of the tag pass)
+  auto dense = [&](int i) -> long long {
+    return (long long)(a.x0 + lane) + (long long)g.W * ((a.y0 + i % TY) + (long long)g.H * (a.z0 + i / TY));
+  };
+  auto is_seed = [&](int i) -> bool {
+    const int x = a.x0 + lane, y = a.y0 + i % TY, z = a.z0 + i / TY;
+    return x < g.W && y < g.H && z < g.D && seeds[dense(i)] == JFC_SEED_FG;
+  };
+  unsigned OBJ[TAG ? R : 1];   // object nodes (tag mode)
+  if constexpr (TAG) {
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const unsigned lb = Lb[roff<TY>(a, i)];
+      OBJ[i] = __ballot_sync(FULL, lb & 1u);
+      NEG[i] = 0u;
+      if constexpr (FIRST) L[i] = __ballot_sync(FULL, is_seed(i));
+      else L[i] = __ballot_sync(FULL, (lb & 2u) != 0);
+    }
+    // a node takes the tag from any tagged neighbour when it is an object node
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int y = i % TY, z = i / TY;
+      IXL[i] = OBJ[i] & ~1u;
+      IXR[i] = OBJ[i] & 0x7fffffffu;
+      IYU[i] = y > 0 ? OBJ[i] : 0u;
+      IYD[i] = y < TY - 1 ? OBJ[i] : 0u;
+      if constexpr (DIMS == 3) {
+        IZU[i] = z > 0 ? OBJ[i] : 0u;
+        IZD[i] = z < TZ - 1 ? OBJ[i] : 0u;
+      }
+    }
+  } else {
     int rxp[R], ryp[R], rym[R], rxm[R], rzp[DIMS == 3 ? R : 1], rzm[DIMS == 3 ? R : 1];
 #pragma unroll
     for (int i = 0; i < R; ++i) {
@@ -160,31 +195,52 @@ __device__ __forceinline__ void cut_tile(const GridDev& g, int4 ti, int tid, con
   }
 #pragma unroll
   for (int i = 0; i < R; ++i) L0[i] = L[i];
-  // sources entering through the halo: neighbour reached and its arc toward us residual
+  // sources entering through the halo: neighbour reached and its arc toward us
+  // residual (cut), or neighbour tagged (tag; the receiving node must be an
+  // object node, applied through the in-masks below)
   auto halo_lab = [&](long long n) -> bool {
-    if constexpr (FIRST) return E[n] > 0;
-    else return Lb[n] != 0;
+    if constexpr (TAG) {
+      if constexpr (FIRST) {
+        const long long x = n % g.pitch, yz = n / g.pitch, y = yz % g.Hp, z = yz / g.Hp;
+        return x < g.W && y < g.H && z < g.D && seeds[x + (long long)g.W * (y + (long long)g.H * z)] == JFC_SEED_FG;
+      } else {
+        return (Lb[n] & 2u) != 0;
+      }
+    } else {
+      if constexpr (FIRST) return E[n] > 0;
+      else return Lb[n] != 0;
+    }
+  };
+  // residual arc from halo node m toward the tile (cut); any neighbour (tag)
+  auto halo_arc = [&](int dir, long long m) -> bool {
+    if constexpr (TAG) return true;
+    else return g.r[dir][m] > 0;
+  };
+  // nodes a halo source may reach: all (cut: the arc decides) or objects (tag)
+  auto objm = [&](int i) -> unsigned {
+    if constexpr (TAG) return OBJ[i];
+    else return FULL;
   };
 #pragma unroll
   for (int z = 0; z < TZ; ++z) {
     const long long n = roff<TY>(a, z * TY);
     bool s = false;
-    if (a.has_yT) { const long long m = n - a.pitch; s = halo_lab(m) && g.r[D::YP][m] > 0; }
-    L[z * TY] |= __ballot_sync(FULL, s);
+    if (a.has_yT) { const long long m = n - a.pitch; s = halo_lab(m) && halo_arc(D::YP, m); }
+    L[z * TY] |= __ballot_sync(FULL, s) & objm(z * TY);
     s = false;
-    if (a.has_yB) { const long long m = n + (long long)TY * a.pitch; s = halo_lab(m) && g.r[D::YM][m] > 0; }
-    L[z * TY + TY - 1] |= __ballot_sync(FULL, s);
+    if (a.has_yB) { const long long m = n + (long long)TY * a.pitch; s = halo_lab(m) && halo_arc(D::YM, m); }
+    L[z * TY + TY - 1] |= __ballot_sync(FULL, s) & objm(z * TY + TY - 1);
   }
   if constexpr (DIMS == 3) {
 #pragma unroll
     for (int y = 0; y < TY; ++y) {
       const long long n = roff<TY>(a, y);
       bool s = false;
-      if (a.has_zT) { const long long m = n - a.slab; s = halo_lab(m) && g.r[D::ZP][m] > 0; }
-      L[y] |= __ballot_sync(FULL, s);
+      if (a.has_zT) { const long long m = n - a.slab; s = halo_lab(m) && halo_arc(D::ZP, m); }
+      L[y] |= __ballot_sync(FULL, s) & objm(y);
       s = false;
-      if (a.has_zB) { const long long m = n + (long long)TZ * a.slab; s = halo_lab(m) && g.r[D::ZM][m] > 0; }
-      L[(TZ - 1) * TY + y] |= __ballot_sync(FULL, s);
+      if (a.has_zB) { const long long m = n + (long long)TZ * a.slab; s = halo_lab(m) && halo_arc(D::ZM, m); }
+      L[(TZ - 1) * TY + y] |= __ballot_sync(FULL, s) & objm((TZ - 1) * TY + y);
     }
   }
   {
@@ -194,13 +250,13 @@ __device__ __forceinline__ void cut_tile(const GridDev& g, int4 ti, int tid, con
     if (row < R && (left ? a.has_xL : a.has_xR)) {
       const long long n = (long long)(left ? a.x0 - 1 : a.x0 + 32) +
                           (long long)(a.y0 + row % TY) * a.pitch + (long long)(a.z0 + row / TY) * a.slab;
-      s = halo_lab(n) && (left ? g.r[D::XP][n] : g.r[D::XM][n]) > 0;
+      s = halo_lab(n) && halo_arc(left ? D::XP : D::XM, n);
     }
     const unsigned sb = __ballot_sync(FULL, s);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
-      L[i] |= (sb >> i) & 1u;
-      L[i] |= ((sb >> (16 + i)) & 1u) << 31;
+      L[i] |= ((sb >> i) & 1u) & objm(i);
+      L[i] |= (((sb >> (16 + i)) & 1u) << 31) & objm(i);
     }
   }
   bool converged = false;
@@ -237,7 +293,14 @@ __device__ __forceinline__ void cut_tile(const GridDev& g, int4 ti, int tid, con
     col0 |= c & 1u;
     col31 |= c >> 31;
     hit |= (L[i] & NEG[i]) != 0u;
-    if (FIRST || c) Lb[roff<TY>(a, i)] = (uint8_t)((L[i] >> lane) & 1u);
+    if constexpr (TAG) {
+      if (FIRST || c) {
+        uint8_t* p = Lb + roff<TY>(a, i);
+        *p = (uint8_t)((*p & 1u) | (((L[i] >> lane) & 1u) << 1));
+      }
+    } else {
+      if (FIRST || c) Lb[roff<TY>(a, i)] = (uint8_t)((L[i] >> lane) & 1u);
+    }
   }
   if (lane == 0 && hit) *bad = 1;
   // boundary labels that differ from what the neighbours last read (their
@@ -249,8 +312,8 @@ __device__ __forceinline__ void cut_tile(const GridDev& g, int4 ti, int tid, con
 // later passes drain the frontier built by the previous one (one tile per
 // warp ticket), grid barriers in between, until a pass queues nothing or the
 // pass budget runs out.
-template <int DIMS, int TY, int TZ>
-__global__ void __launch_bounds__(256) k_cut(TileSet ts, int max_passes) {
+template <int DIMS, int TY, int TZ, bool TAG = false>
+__global__ void __launch_bounds__(256) k_cut(TileSet ts, int max_passes, const uint8_t* seeds) {
   DevCounters* ctr = ts.d_ctr;
   const int lane = threadIdx.x & 31;
   unsigned long long visits = 0;
@@ -266,7 +329,7 @@ __global__ void __launch_bounds__(256) k_cut(TileSet ts, int max_passes) {
       for (int k = 0; k < cnt; ++k) {
         const int tt = (int)b + k;
         const int4 ti = ts.d_info[tt];
-        cut_tile<DIMS, TY, TZ, true>(ts.d_desc[ti.x], ti, tt, Q, &ctr->cut_bad);
+        cut_tile<DIMS, TY, TZ, true, TAG>(ts.d_desc[ti.x], ti, tt, Q, &ctr->cut_bad, seeds);
         ++visits;
       }
     }
@@ -290,7 +353,7 @@ __global__ void __launch_bounds__(256) k_cut(TileSet ts, int max_passes) {
       if (lane == 0) fcur[tt] = 0;
       __syncwarp();
       const int4 ti = ts.d_info[tt];
-      cut_tile<DIMS, TY, TZ, false>(ts.d_desc[ti.x], ti, tt, Q, &ctr->cut_bad);
+      cut_tile<DIMS, TY, TZ, false, TAG>(ts.d_desc[ti.x], ti, tt, Q, &ctr->cut_bad, seeds);
       ++visits;
     }
     ok = jfc::grid_sync(ctr, [&]() {
@@ -915,11 +978,14 @@ __global__ void __launch_bounds__(256) k_grid_sums(const GridDev* __restrict__ g
   }
 }
 
-template <int DIMS, int TY, int TZ, bool CUT>
-cudaError_t bfs_t(const TileSet& ts, int max_passes, cudaStream_t s) {
+// MODE 0: global relabel, 1: cut, 2: tag
+template <int DIMS, int TY, int TZ, int MODE>
+cudaError_t bfs_t(const TileSet& ts, int max_passes, const uint8_t* seeds, cudaStream_t s) {
+  constexpr bool CUT = MODE != 0;
   // global relabel frontier passes: CTA per tile in 2D, warp per tile in 3D
   const void* fn;
-  if constexpr (CUT) fn = (const void*)k_cut<DIMS, TY, TZ>;
+  if constexpr (MODE == 1) fn = (const void*)k_cut<DIMS, TY, TZ, false>;
+  else if constexpr (MODE == 2) fn = (const void*)k_cut<DIMS, TY, TZ, true>;
   else if constexpr (DIMS == 2) fn = (const void*)k_relabel_cta<DIMS, TY, TZ>;
   else fn = (const void*)k_relabel_warp<DIMS, TY, TZ>;
   const int nt = (CUT || DIMS == 3) ? 256 : RTile<DIMS, TY, TZ>::NT;
@@ -933,7 +999,7 @@ cudaError_t bfs_t(const TileSet& ts, int max_passes, cudaStream_t s) {
     if (e != cudaSuccess) return e;
   }
   TileSet arg = ts;
-  void* params[] = {(void*)&arg, (void*)&max_passes};
+  void* params[] = {(void*)&arg, (void*)&max_passes, (void*)&seeds};   // relabel kernels take two
   jfc_note_launch();
   return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(nt), params, 0, s);
 }
@@ -1030,8 +1096,11 @@ int persistent_blocks(const void* kernel, int threads, size_t smem) {
   return sms * per;
 }
 
-cudaError_t launch_bfs(const TileSet& ts, bool cut, int max_passes, cudaStream_t s) {
-#define JFC_BFS(D, Y, Z) (cut ? bfs_t<D, Y, Z, true>(ts, max_passes, s) : bfs_t<D, Y, Z, false>(ts, max_passes, s))
+static cudaError_t bfs_dispatch(const TileSet& ts, int mode, int max_passes, const uint8_t* seeds, cudaStream_t s) {
+#define JFC_BFS(D, Y, Z)                                                       \
+  (mode == 1 ? bfs_t<D, Y, Z, 1>(ts, max_passes, seeds, s)                     \
+             : mode == 2 ? bfs_t<D, Y, Z, 2>(ts, max_passes, seeds, s)         \
+                         : bfs_t<D, Y, Z, 0>(ts, max_passes, seeds, s))
   if (ts.dims == 2) {
     if (ts.TR == 8) return JFC_BFS(2, 8, 1);
     if (ts.TR == 16) return JFC_BFS(2, 16, 1);
@@ -1044,6 +1113,14 @@ cudaError_t launch_bfs(const TileSet& ts, bool cut, int max_passes, cudaStream_t
   if (ts.TY == 8 && ts.TZ == 1) return JFC_BFS(3, 8, 1);
 #undef JFC_BFS
   return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_bfs(const TileSet& ts, bool cut, int max_passes, cudaStream_t s) {
+  return bfs_dispatch(ts, cut ? 1 : 0, max_passes, nullptr, s);
+}
+
+cudaError_t launch_tag(const TileSet& ts, const uint8_t* d_seeds, int max_passes, cudaStream_t s) {
+  return bfs_dispatch(ts, 2, max_passes, d_seeds, s);
 }
 
 cudaError_t launch_grid_sums(const TileSet& ts, cudaStream_t s) {

@@ -53,6 +53,22 @@ __global__ void __launch_bounds__(256) k_energy(int dims, int w, int h, int d, c
 
 }  // namespace
 
+namespace {
+__global__ void k_and_bytes(uint8_t* p, long long n, uint8_t keep) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] &= keep;
+}
+}  // namespace
+
+cudaError_t launch_and_bytes(uint8_t* p, long long n, uint8_t keep, cudaStream_t s) {
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  jfc_note_launch();
+  k_and_bytes<<<(unsigned)blocks, 256, 0, s>>>(p, n, keep);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_energy(int dims, int w, int h, int d, const int32_t* e, const int32_t* const* caps,
                           const uint8_t* lab, unsigned long long* out, cudaStream_t s) {
   Caps c{};

@@ -528,6 +528,43 @@ int jfc_edit_tlinks(jfc_graph* G, const uint32_t* idx, const int32_t* dcs, const
   return JFC_OK;
 }
 
+int jfc_graph_compute_tag(jfc_graph* G, const uint8_t* seeds, uint8_t* tag) {
+  if (!G || !tag) return set_error(JFC_ERR_INVALID_ARG, "null argument");
+  if (G->state != 2) return set_error(JFC_ERR_STATE, "not solved");
+  if (!seeds && !G->model.valid) return set_error(JFC_ERR_STATE, "no seeds: graph was not built from an image");
+  JFC_CUDA(cudaSetDevice(G->ctx->device));
+  int rc = ensure_tileset(G);
+  if (rc) return rc;
+  cudaStream_t s = G->ctx->stream;
+  const size_t n = (size_t)G->W * G->H * G->D;
+  uint8_t* d_seeds = G->model.valid && !seeds ? G->model.d_seeds : nullptr;
+  uint8_t* d_tmp = nullptr;
+  if (seeds) {
+    JFC_CUDA(cudaMallocAsync((void**)&d_tmp, n, s));
+    d_seeds = d_tmp;
+  }
+  TileSet& ts = G->ts;
+  DevCounters hc;
+  cudaError_t e = seeds ? cudaMemcpyAsync(d_tmp, seeds, n, cudaMemcpyHostToDevice, s) : cudaSuccess;
+  if (e == cudaSuccess) e = cudaMemsetAsync(ts.d_flag_bfs[0], 0, sizeof(int) * (size_t)ts.ntiles, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ts.d_flag_bfs[1], 0, sizeof(int) * (size_t)ts.ntiles, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ts.d_ctr->qn_bfs, 0, sizeof(ts.d_ctr->qn_bfs), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(&ts.d_ctr->bfs_status, 0, sizeof(int), s);
+  if (e == cudaSuccess) e = launch_tag(ts, d_seeds, G->ctx->params.max_bfs_passes, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hc, ts.d_ctr, sizeof(hc), cudaMemcpyDeviceToHost, s);
+  // tags leave in bit 1 of the label plane; the plane is restored afterwards
+  if (e == cudaSuccess) e = copy_plane(G->g.label, tag, 1, G, true, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = launch_and_bytes(G->g.label, G->g.plane, 1, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (d_tmp) cudaFreeAsync(d_tmp, s);
+  if (e != cudaSuccess) return cuda_status(e, "tag");
+  if (hc.error) return set_error(JFC_ERR_CUDA, "grid barrier timed out in a persistent kernel");
+  if (hc.bfs_status == 2) return set_error(JFC_ERR_NOT_CONVERGED, "BFS pass budget exhausted");
+  for (size_t i = 0; i < n; ++i) tag[i] = (tag[i] >> 1) & 1u;
+  return JFC_OK;
+}
+
 int jfc_energy_device(int device, void* stream, int dims, int w, int h, int d, const int32_t* d_excess,
                       const int32_t* const* d_ncap, const uint8_t* d_labels, int64_t* data, int64_t* smooth) {
   if (!d_excess || !d_ncap || !d_labels || !data || !smooth) return set_error(JFC_ERR_INVALID_ARG, "null argument");

@@ -152,6 +152,7 @@ def _lib():
         L.jfc_server_close.argtypes = [VP, ctypes.c_int]
         L.jfc_server_cancel.argtypes = [VP, ctypes.c_int]
         L.jfc_server_get_stats.argtypes = [VP, ctypes.POINTER(ServerStats)]
+        L.jfc_graph_compute_tag.argtypes = [VP, U8P, U8P]
         L.jfc_energy_device.argtypes = [ctypes.c_int, VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         VP, ctypes.POINTER(VP), VP, ctypes.POINTER(ctypes.c_int64),
                                         ctypes.POINTER(ctypes.c_int64)]
@@ -301,6 +302,14 @@ class Graph:
         _check(_lib().jfc_graph_set(self.handle, _p(e, I32P), P, int(flow_offset)), "jfc_graph_set")
 
     slotLoadGraphClicked = set
+
+    def tag(self, seeds=None):
+        """Object nodes connected to a foreground seed (the reference's tag pass)."""
+        out = np.empty(self.n, np.uint8)
+        sp = None if seeds is None else np.ascontiguousarray(seeds, np.uint8).ravel()
+        _check(_lib().jfc_graph_compute_tag(self.handle, None if sp is None else _p(sp, U8P), _p(out, U8P)),
+               "jfc_graph_compute_tag")
+        return out.reshape(self.shape)
 
     def load_files(self, base):
         """Load <base>.ef/.c1/.c2 (the reference's graph files) into this grid."""

@@ -409,6 +409,48 @@ def test_energy_certificate(ctx):
         g.close()
 
 
+def _tag_oracle(obj, fg):
+    """Object nodes connected through object nodes to a foreground seed (plus
+    the seeds), by repeated 4/6-neighbour dilation."""
+    tag = fg.copy()
+    while True:
+        grow = tag.copy()
+        for ax in range(obj.ndim):
+            for sh in (1, -1):
+                rolled = np.roll(tag, sh, axis=ax)
+                idx = [slice(None)] * obj.ndim
+                idx[ax] = 0 if sh == 1 else -1
+                rolled[tuple(idx)] = False
+                grow |= rolled & obj
+        if np.array_equal(grow, tag):
+            return tag
+        tag = grow
+
+
+def test_tag_post_process(ctx):
+    img, seeds = jfcut.synth_gray_ellipse(300, 200, seed=21)
+    g = jfcut.Graph(ctx, seeds.shape)
+    g.build_from_image(img, seeds, jfcut.PIX_GRAY8, MODEL2)
+    g.solve()
+    lab = g.labels().copy()
+    tag = g.tag()
+    want = _tag_oracle(lab.astype(bool), seeds == jfcut.SEED_FG)
+    assert np.array_equal(tag.astype(bool), want)
+    assert np.array_equal(g.labels(), lab)          # labels untouched
+    # explicit seeds on a graph given as arrays, 3D
+    rng = np.random.default_rng(77)
+    shp = (6, 17, 40)
+    e, caps = random_grid(shp, rng, cap_max=30, density=0.5)
+    g3, _ = solve_set(ctx, shp, e, caps)
+    lab3 = g3.labels().reshape(shp).astype(bool)
+    fg = np.zeros(shp, np.uint8)
+    fg.ravel()[rng.choice(fg.size, 25, replace=False)] = jfcut.SEED_FG
+    tag3 = g3.tag(fg)
+    assert np.array_equal(tag3.astype(bool), _tag_oracle(lab3, fg == jfcut.SEED_FG))
+    g.close()
+    g3.close()
+
+
 def test_errors(ctx):
     img, seeds = jfcut.synth_gray_ellipse(64, 64, seed=1)
     g = jfcut.Graph(ctx, img.shape)

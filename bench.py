@@ -35,6 +35,19 @@ MODEL = dict(lambda_n=100, z_weight_pct=100, lambda_t=10, k_fg=5, k_bg=5, seed_c
 METRIC = "Mnodes/s to exact min-cut (plain, 2D 4-conn 15000x10000 RGB)"
 
 
+def pr_traffic_per_launch():
+    """DRAM bytes per push-relabel phase launch from the committed ncu capture
+    of this workload (profiles/k_pr_phase_traffic_15000x10000.md), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "k_pr_phase_traffic_15000x10000.md")) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -543,6 +556,7 @@ def main():
     bytes_per_visit = 32 * tr * 48 + (2 * 32 + 2 * tr) * 12
     achieved = visits * bytes_per_visit / (ms_pr / 1000.0) / 1e9 if ms_pr > 0 else 0.0
     peak, peak_kind = peaks()
+    pr_launches = int(agg["global_relabels"]) - args.steps    # one phase per relabel cycle
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Mnodes/s", "n_gpus": world, "steps": args.steps,
@@ -561,8 +575,12 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clk,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "kernel": "k_pr_sweep (push-relabel tile visits; %d B/visit algorithmic, %s peak)"
+                         "frac": achieved / peak,
+                         "traffic": pr_traffic_per_launch() if (w, h) == (W_FULL, H_FULL) else None,
+                         "algorithmic_bytes_per_launch": visits * bytes_per_visit / max(1, pr_launches),
+                         "launches": pr_launches,
+                         "kernel": "k_pr_phase (push-relabel phases; %d B per tile visit algorithmic, %s peak; "
+                                   "traffic from the committed ncu capture of this workload)"
                                    % (bytes_per_visit, peak_kind)},
         }
         if world == 1 and not args.no_cpu_baseline:

@@ -29,6 +29,7 @@
 // the launches (tests check alone vs in the mix).
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -99,7 +100,7 @@ struct jfc_server {
   int solving = 0, peak_solving = 0;
   long long loops = 0, requests_done = 0;
 
-  TileSet ts[2], cut_ts[2];         // solving set / converged grids, [0] 2D, [1] 3D
+  TileSet cut_ts[2];                // converged grids of a cycle, [0] 2D, [1] 3D
 };
 
 namespace {
@@ -200,74 +201,192 @@ struct Member {
   bool done = false;      // result delivered; leaves at the next membership change
 };
 
-void solver_loop(jfc_server* S) {
-  cudaSetDevice(S->device);
-  jfc_ctx* ctx = S->solve_ctx;
-  const jfc_params& p = S->params;
+// A solving set: one tile set per dimensionality over its members' grids.
+// The server runs two: interactive (warm stroke edits) and bulk (cold
+// requests); the interactive lane gets its cycles first, so an edit does not
+// wait behind the relabels of large cold solves.
+struct Lane {
   std::vector<Member> mem[2];       // members of ts[0] / ts[1], in grid order
   std::vector<int> active[2];       // active tiles per grid after the last relabel
-  int interval = p.relabel_interval;
-  auto fail_all = [&](int rc) {
-    std::lock_guard<std::mutex> lk(S->mu);
-    S->fatal = rc;
-    const Clock::time_point now = Clock::now();
+  TileSet ts[2];
+  int interval = 4;
+  std::vector<Session*> joining;    // admitted requests, join at the next relabel
+  std::vector<Session*> freeing;    // closed members, freed once ts[] no longer holds them
+  bool empty() const { return mem[0].empty() && mem[1].empty() && joining.empty(); }
+  long long active_tiles() const {
+    long long a = 0;
     for (int k = 0; k < 2; ++k)
-      for (Member& m : mem[k]) {
-        if (!m.done) finish_front(S, m.s, rc, 0, now);
-        cancel_all(S, m.s, now);
-        m.s->phase = IDLE;
-      }
-    S->cv_done.notify_all();
-  };
-  for (;;) {
-    // 1. push-relabel phase over the current solving set
-    long long total_active = 0;
-    for (int k = 0; k < 2; ++k)
-      for (size_t i = 0; i < mem[k].size(); ++i)
-        if (!mem[k][i].done) total_active += active[k][i];
-    bool ran_pr[2] = {false, false};
-    for (int k = 0; k < 2; ++k) {
-      long long a = 0;
       for (size_t i = 0; i < mem[k].size(); ++i)
         if (!mem[k][i].done) a += active[k][i];
-      if (a == 0) continue;
-      cudaMemsetAsync(S->ts[k].d_ctr->ticket, 0, sizeof(S->ts[k].d_ctr->ticket), ctx->stream);
-      const cudaError_t e = launch_pr_phase(S->ts[k], interval, p.local_iters, ctx->stream);
-      if (e != cudaSuccess) { fail_all(cuda_status(e, "push-relabel phase")); return; }
-      ran_pr[k] = true;
+    return a;
+  }
+};
+
+// Finish every request of the lane's members with a device error.
+void fail_lane(jfc_server* S, Lane& L, int rc) {
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->fatal = rc;
+  const Clock::time_point now = Clock::now();
+  for (int k = 0; k < 2; ++k)
+    for (Member& m : L.mem[k]) {
+      if (!m.done) finish_front(S, m.s, rc, 0, now);
+      cancel_all(S, m.s, now);
+      m.s->phase = IDLE;
     }
-    // 2. membership: leave (done / cancelled), free closed sessions, join
-    bool changed[2] = {false, false};
-    std::vector<Session*> joining, frees;
+  S->cv_done.notify_all();
+}
+
+// One relabel cycle of a lane: push-relabel phase over its members, then
+// membership (leave / join), then one global relabel over the re-formed set,
+// then the cut of every converged grid.  Returns a status (device errors).
+int lane_cycle(jfc_server* S, Lane& L) {
+  jfc_ctx* ctx = S->solve_ctx;
+  const jfc_params& p = S->params;
+  // 1. push-relabel phase over the current members
+  bool ran_pr[2] = {false, false};
+  for (int k = 0; k < 2; ++k) {
+    long long a = 0;
+    for (size_t i = 0; i < L.mem[k].size(); ++i)
+      if (!L.mem[k][i].done) a += L.active[k][i];
+    if (a == 0) continue;
+    cudaMemsetAsync(L.ts[k].d_ctr->ticket, 0, sizeof(L.ts[k].d_ctr->ticket), ctx->stream);
+    const cudaError_t e = launch_pr_phase(L.ts[k], L.interval, p.local_iters, ctx->stream);
+    if (e != cudaSuccess) return cuda_status(e, "push-relabel phase");
+    ran_pr[k] = true;
+  }
+  // 2. membership: done / cancelled members leave, admitted requests join
+  bool changed[2] = {false, false};
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    const Clock::time_point now = Clock::now();
+    for (int k = 0; k < 2; ++k) {
+      std::vector<Member> keep;
+      std::vector<int> keep_act;
+      for (size_t i = 0; i < L.mem[k].size(); ++i) {
+        Member& m = L.mem[k][i];
+        if (!m.done && m.s->cancel) {
+          cancel_all(S, m.s, now);
+          m.s->phase = IDLE;
+          m.done = true;
+          S->cv_done.notify_all();
+        }
+        if (m.done) {
+          changed[k] = true;
+          if (m.s->close) L.freeing.push_back(m.s);
+          continue;
+        }
+        keep.push_back(m);
+        keep_act.push_back(L.active[k][i]);
+      }
+      L.mem[k].swap(keep);
+      L.active[k].swap(keep_act);
+    }
+  }
+  for (Session* s : L.joining) {
+    const int k = s->dims == 3 ? 1 : 0;
+    L.mem[k].push_back(Member{s});
+    L.active[k].push_back(0);
+    changed[k] = true;
+  }
+  L.joining.clear();
+  // 3. global relabel over the (re-formed) set
+  for (int k = 0; k < 2; ++k) {
+    if (L.mem[k].empty()) {
+      L.active[k].clear();
+      continue;
+    }
+    if (changed[k]) {
+      std::vector<GridDev> grids;
+      for (Member& m : L.mem[k]) grids.push_back(m.s->G->g);
+      int rc = tileset_build(L.ts[k], k ? 3 : 2, p.tile_rows, p.tile_depth, grids, ctx->stream);
+      if (rc) return rc;
+    }
+    int passes = 0, sw = 0;
+    int rc = engine_bfs(ctx, L.ts[k], p, false, passes, &L.active[k], nullptr, &sw);
+    if (rc) return rc;
+    if (ran_pr[k])
+      for (Member& m : L.mem[k]) m.s->sweeps += sw;
+  }
+  // closed members are no longer in any tile set of this lane (rebuilt above,
+  // or the lane is empty and launches nothing): free their device state
+  for (Session* s : L.freeing) {
+    free_session(S, s);
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->sessions.erase(s->sid);
+  }
+  L.freeing.clear();
+  // 4. converged grids: cut BFS on a tile set of those grids alone
+  long long still = 0;
+  for (int k = 0; k < 2; ++k) {
+    std::vector<size_t> conv;
+    for (size_t i = 0; i < L.mem[k].size(); ++i) {
+      if (L.active[k][i] == 0) conv.push_back(i);
+      else if (L.mem[k][i].s->sweeps >= p.max_sweeps) conv.push_back(i);
+      else still += L.active[k][i];
+    }
+    if (conv.empty()) continue;
+    std::vector<GridDev> grids;
+    for (size_t i : conv) grids.push_back(L.mem[k][i].s->G->g);
+    int rc = tileset_build(S->cut_ts[k], k ? 3 : 2, p.tile_rows, p.tile_depth, grids, ctx->stream);
+    if (rc) return rc;
+    std::vector<GridResult> res;
+    int passes = 0;
+    rc = engine_cut(ctx, S->cut_ts[k], p, res, passes);
+    if (rc && rc != JFC_ERR_NOT_CONVERGED) return rc;
+    std::lock_guard<std::mutex> lk(S->mu);
+    const Clock::time_point now = Clock::now();
+    for (size_t j = 0; j < conv.size(); ++j) {
+      Member& m = L.mem[k][conv[j]];
+      Session* s = m.s;
+      jfc_graph* G = s->G;
+      int st = res[j].status;
+      if (L.active[k][conv[j]] > 0) st = JFC_ERR_NOT_CONVERGED;
+      G->flow = G->sink_total + res[j].neg_sum;
+      G->source_nodes = res[j].labels;
+      G->state = st == JFC_OK ? 2 : 1;
+      finish_front(S, s, st, G->flow, now);
+      m.done = true;
+      if (s->cancel) cancel_all(S, s, now);
+      if (!s->reqs.empty() && !s->close) {
+        s->phase = READY;
+        S->ready_q.push_back(s->sid);
+      } else {
+        s->phase = IDLE;
+      }
+    }
+    S->cv_done.notify_all();
+  }
+  // adaptive interval as in the plain solve: a sliver of active tiles makes
+  // the dense relabel dominate, so relabel less often
+  const long long nt = (long long)L.ts[0].ntiles * (L.mem[0].empty() ? 0 : 1) +
+                       (long long)L.ts[1].ntiles * (L.mem[1].empty() ? 0 : 1);
+  if (p.verbose)
+    fprintf(stderr, "{\"lane_cycle\": %d, \"members\": %zu, \"active_tiles\": %lld, \"tiles\": %lld, \"interval\": %d}\n",
+            (int)(&L - &L), L.mem[0].size() + L.mem[1].size(), still, nt, L.interval);
+  if (still > 0 && still * 256 < nt) L.interval = std::min(L.interval * 2, p.relabel_interval_max);
+  else L.interval = p.relabel_interval;
+  return JFC_OK;
+}
+
+void solver_loop(jfc_server* S) {
+  cudaSetDevice(S->device);
+  const jfc_params& p = S->params;
+  Lane lanes[2];                    // [0] interactive (warm edits), [1] bulk (cold)
+  lanes[0].interval = lanes[1].interval = p.relabel_interval;
+  constexpr int kInteractiveCycles = 16;   // interactive cycles per bulk cycle, at most
+  for (;;) {
+    // admission: requests waiting for a slot join their lane at its next relabel
+    std::vector<Session*> admitted, frees;
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      if (total_active == 0 && mem[0].empty() && mem[1].empty())
+      if (lanes[0].empty() && lanes[1].empty())
         S->cv_work.wait(lk, [&] { return S->stop || !S->ready_q.empty() || !S->to_free.empty(); });
       if (S->stop) break;
       const Clock::time_point now = Clock::now();
-      for (int k = 0; k < 2; ++k) {
-        std::vector<Member> keep;
-        std::vector<int> keep_act;
-        for (size_t i = 0; i < mem[k].size(); ++i) {
-          Member& m = mem[k][i];
-          if (!m.done && m.s->cancel) {
-            cancel_all(S, m.s, now);
-            m.done = true;
-            S->cv_done.notify_all();
-          }
-          if (m.done) {
-            changed[k] = true;
-            if (m.s->close) S->to_free.push_back(m.s);
-            continue;
-          }
-          keep.push_back(m);
-          keep_act.push_back(active[k][i]);
-        }
-        mem[k].swap(keep);
-        active[k].swap(keep_act);
-      }
-      frees.swap(S->to_free);
-      int slots = S->max_slots - (int)(mem[0].size() + mem[1].size());
+      frees.swap(S->to_free);   // idle sessions: in no lane
+      int members = 0;
+      for (Lane& L : lanes) members += (int)(L.mem[0].size() + L.mem[1].size() + L.joining.size());
+      int slots = S->max_slots - members;
       while (slots > 0 && !S->ready_q.empty()) {
         Session* s = S->sessions.at(S->ready_q.front()).get();
         S->ready_q.pop_front();
@@ -280,108 +399,58 @@ void solver_loop(jfc_server* S) {
         }
         s->phase = SOLVING;
         if (!s->reqs.front().cold) s->reqs.front().t_admit = now;
-        joining.push_back(s);
+        admitted.push_back(s);
         --slots;
       }
+      ++S->loops;
     }
     for (Session* s : frees) {
       free_session(S, s);
       std::lock_guard<std::mutex> lk(S->mu);
       S->sessions.erase(s->sid);
     }
-    // a label read in progress finishes before any joining edit changes a graph
-    std::unique_lock<std::mutex> rl(S->read_mu, std::defer_lock);
-    if (!joining.empty()) rl.lock();
-    for (Session* s : joining) {
-      int rc = JFC_OK;
-      Request& r = s->reqs.front();
-      if (!r.cold) rc = jfc_graph_edit_seeds(s->G, r.idx.data(), r.seed.data(), r.idx.size());
-      if (rc != JFC_OK) {
-        std::lock_guard<std::mutex> lk(S->mu);
-        finish_front(S, s, rc, 0, Clock::now());
-        s->phase = s->reqs.empty() ? IDLE : READY;
-        if (!s->reqs.empty()) S->ready_q.push_back(s->sid);
-        S->cv_done.notify_all();
-        continue;
+    if (!admitted.empty()) {
+      // a label read in progress finishes before an edit changes a graph
+      std::lock_guard<std::mutex> rl(S->read_mu);
+      for (Session* s : admitted) {
+        Request& r = s->reqs.front();
+        int rc = JFC_OK;
+        if (!r.cold) rc = jfc_graph_edit_seeds(s->G, r.idx.data(), r.seed.data(), r.idx.size());
+        if (rc != JFC_OK) {
+          std::lock_guard<std::mutex> lk(S->mu);
+          finish_front(S, s, rc, 0, Clock::now());
+          s->phase = s->reqs.empty() ? IDLE : READY;
+          if (!s->reqs.empty()) S->ready_q.push_back(s->sid);
+          S->cv_done.notify_all();
+          continue;
+        }
+        lanes[r.cold ? 1 : 0].joining.push_back(s);
       }
-      const int k = s->dims == 3 ? 1 : 0;
-      mem[k].push_back(Member{s});
-      active[k].push_back(0);
-      changed[k] = true;
     }
-    if (rl.owns_lock()) rl.unlock();
     {
       std::lock_guard<std::mutex> lk(S->mu);
-      ++S->loops;
-      S->solving = (int)(mem[0].size() + mem[1].size());
-      S->peak_solving = std::max(S->peak_solving, S->solving);
+      int solving = 0;
+      for (Lane& L : lanes) solving += (int)(L.mem[0].size() + L.mem[1].size() + L.joining.size());
+      S->solving = solving;
+      S->peak_solving = std::max(S->peak_solving, solving);
     }
-    // 3. global relabel over the (re-formed) solving set
-    for (int k = 0; k < 2; ++k) {
-      if (mem[k].empty()) {
-        active[k].clear();
-        continue;
+    // interactive lane first (until it drains, bounded), then one bulk cycle
+    for (int c = 0; c < kInteractiveCycles && !lanes[0].empty(); ++c) {
+      const int rc = lane_cycle(S, lanes[0]);
+      if (rc) { fail_lane(S, lanes[0], rc); fail_lane(S, lanes[1], rc); return; }
+      if (lanes[0].active_tiles() == 0 && lanes[0].joining.empty()) {
+        // converged members leave at the next cycle; run it now only if
+        // someone is waiting for a slot
+        break;
       }
-      if (changed[k]) {
-        std::vector<GridDev> grids;
-        for (Member& m : mem[k]) grids.push_back(m.s->G->g);
-        int rc = tileset_build(S->ts[k], k ? 3 : 2, p.tile_rows, p.tile_depth, grids, ctx->stream);
-        if (rc) { fail_all(rc); return; }
-      }
-      int passes = 0, sw = 0;
-      int rc = engine_bfs(ctx, S->ts[k], p, false, passes, &active[k], nullptr, &sw);
-      if (rc) { fail_all(rc); return; }
-      if (ran_pr[k])
-        for (Member& m : mem[k]) m.s->sweeps += sw;
     }
-    // 4. converged grids: cut BFS on a tile set of those grids alone
-    long long still = 0;
-    for (int k = 0; k < 2; ++k) {
-      std::vector<size_t> conv;
-      for (size_t i = 0; i < mem[k].size(); ++i) {
-        if (active[k][i] == 0) conv.push_back(i);
-        else if (mem[k][i].s->sweeps >= p.max_sweeps) conv.push_back(i);
-        else still += active[k][i];
-      }
-      if (conv.empty()) continue;
-      std::vector<GridDev> grids;
-      for (size_t i : conv) grids.push_back(mem[k][i].s->G->g);
-      int rc = tileset_build(S->cut_ts[k], k ? 3 : 2, p.tile_rows, p.tile_depth, grids, ctx->stream);
-      if (rc) { fail_all(rc); return; }
-      std::vector<GridResult> res;
-      int passes = 0;
-      rc = engine_cut(ctx, S->cut_ts[k], p, res, passes);
-      if (rc && rc != JFC_ERR_NOT_CONVERGED) { fail_all(rc); return; }
-      std::lock_guard<std::mutex> lk(S->mu);
-      const Clock::time_point now = Clock::now();
-      for (size_t j = 0; j < conv.size(); ++j) {
-        Member& m = mem[k][conv[j]];
-        Session* s = m.s;
-        jfc_graph* G = s->G;
-        int st = res[j].status;
-        if (active[k][conv[j]] > 0) st = JFC_ERR_NOT_CONVERGED;
-        G->flow = G->sink_total + res[j].neg_sum;
-        G->source_nodes = res[j].labels;
-        G->state = st == JFC_OK ? 2 : 1;
-        finish_front(S, s, st, G->flow, now);
-        m.done = true;
-        if (s->cancel) cancel_all(S, s, now);
-        if (!s->reqs.empty() && !s->close) {
-          s->phase = READY;
-          S->ready_q.push_back(s->sid);
-        } else {
-          s->phase = IDLE;
-        }
-      }
-      S->cv_done.notify_all();
+    if (!lanes[1].empty()) {
+      const int rc = lane_cycle(S, lanes[1]);
+      if (rc) { fail_lane(S, lanes[0], rc); fail_lane(S, lanes[1], rc); return; }
     }
-    // adaptive interval as in the plain solve: a sliver of active tiles
-    // makes the dense relabel dominate, so relabel less often
-    long long nt = (long long)S->ts[0].ntiles * (mem[0].empty() ? 0 : 1) +
-                   (long long)S->ts[1].ntiles * (mem[1].empty() ? 0 : 1);
-    if (still > 0 && still * 256 < nt) interval = std::min(interval * 2, p.relabel_interval_max);
-    else interval = p.relabel_interval;
   }
+  for (Lane& L : lanes)
+    for (int k = 0; k < 2; ++k) tileset_free(L.ts[k]);
 }
 
 Session* find(jfc_server* S, int sid) {
@@ -436,10 +505,7 @@ void jfc_server_destroy(jfc_server* S) {
   S->builder.join();
   S->solver.join();
   cudaSetDevice(S->device);
-  for (int k = 0; k < 2; ++k) {
-    tileset_free(S->ts[k]);
-    tileset_free(S->cut_ts[k]);
-  }
+  for (int k = 0; k < 2; ++k) tileset_free(S->cut_ts[k]);
   for (auto& kv : S->sessions)
     if (kv.second->G) jfc_graph_destroy(kv.second->G);
   S->sessions.clear();

@@ -308,6 +308,18 @@ int jfc_create(int device, const jfc_params* params, jfc_ctx** out) {
   if (params) c->params = *params;
   else jfc_default_params(&c->params);
   fill_defaults(c->params);
+  {
+    // stream-ordered temporaries (capacity build, edits) come from the
+    // device's default pool: keep up to 1 GiB of freed blocks mapped instead
+    // of returning them at every synchronisation
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = 1ull << 30, cur = 0;
+      if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess && cur < keep)
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+  }
   e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete c; return cuda_status(e, "cudaStreamCreate"); }
   c->stream = c->own_stream;

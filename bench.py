@@ -282,13 +282,13 @@ def bench_batched(jfcut, torch, ctx, stream, steps, warmup, n_inst=256):
     return out
 
 
-def bench_video(jfcut, torch, ctx, stream, steps=2, warmup=1):
+def bench_video(jfcut, torch, ctx, stream, steps=2, warmup=1, size=(2560, 1440, 50)):
     """3D plain workload: 6-connected 2560x1440x50 RGB video (184M nodes), an
     ellipse moving 4 px/frame over seeded value-noise texture, temporal n-link
     weight 0.5x the spatial one, 5-means colour models, strokes on frames 0
     and 49.  One step = capacity build from device-resident frames + solve +
     labels into a device buffer; flows must repeat exactly."""
-    w, h, d = 2560, 1440, 50
+    w, h, d = size
     img, seeds = jfcut.synth_rgb_video(w, h, d, seed=SEED + 50)
     model = dict(MODEL, z_weight_pct=50)
     d_img = torch.from_numpy(img).cuda()
@@ -312,7 +312,7 @@ def bench_video(jfcut, torch, ctx, stream, steps=2, warmup=1):
     g.close()
     n = w * h * d
     m = float(np.mean(ms))
-    return {"workload": "3D 6-conn 2560x1440x50 RGB video (build + solve + labels per step)", "nodes": n,
+    return {"workload": "3D 6-conn %dx%dx%d RGB video (build + solve + labels per step)" % (w, h, d), "nodes": n,
             "ms_per_step": m, "mnodes_s": n / (m / 1e3) / 1e6, "flow": flows.pop() if len(flows) == 1 else None,
             "flow_repeatable": len(flows) <= 1,
             "solve_breakdown": {k: round(getattr(agg, k), 2) for k in
@@ -457,6 +457,7 @@ def main():
     ap.add_argument("--extras", default="video,batched,edit4096,serve",
                     help="comma list of extra sections at N=1 (video, batched, edit4096, serve) or 'none'")
     ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--video-size", default="2560x1440x50", help="WxHxD of the video section")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -586,7 +587,8 @@ def main():
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_bk()
         extras = [] if world > 1 or args.extras == "none" else args.extras.split(",")
-        sections = {"video": lambda: bench_video(jfcut, torch, ctx, stream),
+        vsize = tuple(int(v) for v in args.video_size.split("x"))
+        sections = {"video": lambda: bench_video(jfcut, torch, ctx, stream, size=vsize),
                     "batched": lambda: bench_batched(jfcut, torch, ctx, stream, 2, 1),
                     "edit4096": lambda: bench_edit4096(jfcut, torch, ctx),
                     "serve": lambda: bench_serve(jfcut, torch, ctx, n_req=args.serve_requests)}

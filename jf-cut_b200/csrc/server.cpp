@@ -239,7 +239,7 @@ void fail_lane(jfc_server* S, Lane& L, int rc) {
 // One relabel cycle of a lane: push-relabel phase over its members, then
 // membership (leave / join), then one global relabel over the re-formed set,
 // then the cut of every converged grid.  Returns a status (device errors).
-int lane_cycle(jfc_server* S, Lane& L) {
+int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
   jfc_ctx* ctx = S->solve_ctx;
   const jfc_params& p = S->params;
   // 1. push-relabel phase over the current members
@@ -361,8 +361,8 @@ int lane_cycle(jfc_server* S, Lane& L) {
   const long long nt = (long long)L.ts[0].ntiles * (L.mem[0].empty() ? 0 : 1) +
                        (long long)L.ts[1].ntiles * (L.mem[1].empty() ? 0 : 1);
   if (p.verbose)
-    fprintf(stderr, "{\"lane_cycle\": %d, \"members\": %zu, \"active_tiles\": %lld, \"tiles\": %lld, \"interval\": %d}\n",
-            (int)(&L - &L), L.mem[0].size() + L.mem[1].size(), still, nt, L.interval);
+    fprintf(stderr, "{\"lane\": \"%s\", \"members\": %zu, \"active_tiles\": %lld, \"tiles\": %lld, \"interval\": %d}\n",
+            lane_id == 0 ? "interactive" : "bulk", L.mem[0].size() + L.mem[1].size(), still, nt, L.interval);
   if (still > 0 && still * 256 < nt) L.interval = std::min(L.interval * 2, p.relabel_interval_max);
   else L.interval = p.relabel_interval;
   return JFC_OK;
@@ -436,7 +436,7 @@ void solver_loop(jfc_server* S) {
     }
     // interactive lane first (until it drains, bounded), then one bulk cycle
     for (int c = 0; c < kInteractiveCycles && !lanes[0].empty(); ++c) {
-      const int rc = lane_cycle(S, lanes[0]);
+      const int rc = lane_cycle(S, lanes[0], 0);
       if (rc) { fail_lane(S, lanes[0], rc); fail_lane(S, lanes[1], rc); return; }
       if (lanes[0].active_tiles() == 0 && lanes[0].joining.empty()) {
         // converged members leave at the next cycle; run it now only if
@@ -445,7 +445,7 @@ void solver_loop(jfc_server* S) {
       }
     }
     if (!lanes[1].empty()) {
-      const int rc = lane_cycle(S, lanes[1]);
+      const int rc = lane_cycle(S, lanes[1], 1);
       if (rc) { fail_lane(S, lanes[0], rc); fail_lane(S, lanes[1], rc); return; }
     }
   }

@@ -320,6 +320,32 @@ def bench_video(jfcut, torch, ctx, stream, steps=2, warmup=1, size=(2560, 1440, 
                                  "global_relabels")}}
 
 
+def bench_fastcut(jfcut, torch, w=4096, h=3072, reps=2):
+    """The reference's Fast-Cut line sweeps (pr_mode 1) against the block-wise
+    push-relabel on a 4096x3072 instance of the plain workload: solve time,
+    sweeps and relabels of each (flows must agree)."""
+    img, seeds = make_workload(w, h, SEED)
+    d_img, d_seeds = torch.from_numpy(img).cuda(), torch.from_numpy(seeds).cuda()
+    out = {"workload": "plain 2D 4-conn %dx%d RGB (solve only)" % (w, h)}
+    flows = set()
+    for name, params in (("block", dict(pr_mode=0)), ("fastcut", dict(pr_mode=1, relabel_interval=2))):
+        ctx = jfcut.Context(0, **params)
+        g = jfcut.Graph(ctx, (h, w))
+        best = None
+        for _ in range(reps):
+            g.build_from_device(d_img.data_ptr(), d_seeds.data_ptr(), jfcut.PIX_RGB8, MODEL)
+            st = g.solve()
+            if best is None or st.ms_total < best.ms_total:
+                best = st
+            flows.add(g.flow())
+        out[name] = {"ms": best.ms_total, "sweeps": best.sweeps, "global_relabels": best.global_relabels}
+        g.close()
+        ctx.close()
+    out["speedup_block_vs_fastcut"] = out["fastcut"]["ms"] / out["block"]["ms"]
+    out["flows_agree"] = len(flows) == 1
+    return out
+
+
 def bench_serve(jfcut, torch, ctx, n_req=48, rate=200.0, budget_gb=96):
     """Serving workload: Poisson arrivals (mean `rate`/s) of n_req sessions,
     70% 2D RGB images (sides U[256,4096], 4-conn) and 30% int16 phantom
@@ -454,8 +480,9 @@ def main():
     ap.add_argument("--width", type=int, default=W_FULL)
     ap.add_argument("--height", type=int, default=H_FULL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--extras", default="video,batched,edit4096,serve",
-                    help="comma list of extra sections at N=1 (video, batched, edit4096, serve) or 'none'")
+    ap.add_argument("--extras", default="video,batched,edit4096,serve,fastcut",
+                    help="comma list of extra sections at N=1 (video, batched, edit4096, serve, fastcut) "
+                         "or 'none'")
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--video-size", default="2560x1440x50", help="WxHxD of the video section")
     args = ap.parse_args()
@@ -591,9 +618,10 @@ def main():
         sections = {"video": lambda: bench_video(jfcut, torch, ctx, stream, size=vsize),
                     "batched": lambda: bench_batched(jfcut, torch, ctx, stream, 2, 1),
                     "edit4096": lambda: bench_edit4096(jfcut, torch, ctx),
+                    "fastcut": lambda: bench_fastcut(jfcut, torch),
                     "serve": lambda: bench_serve(jfcut, torch, ctx, n_req=args.serve_requests)}
         with torch.cuda.stream(stream):
-            for name in ("video", "batched", "edit4096", "serve"):
+            for name in ("video", "batched", "edit4096", "serve", "fastcut"):
                 if name in extras:
                     t0 = time.perf_counter()
                     try:

@@ -58,6 +58,7 @@ void fill_defaults(jfc_params& p) {
   // 3D tile depth: 0 = automatic (32 x 4 x 2 tiles); 4 needs tile_rows 16
   if (p.tile_depth == 4 && p.tile_rows == 8) p.tile_depth = 2;
   if (p.tile_depth != 1 && p.tile_depth != 2 && p.tile_depth != 4) p.tile_depth = 0;
+  if (p.pr_mode != 1) p.pr_mode = 0;
   if (p.local_iters <= 0) p.local_iters = 16;
   if (p.relabel_interval <= 0) p.relabel_interval = 4;
   if (p.relabel_interval_max < p.relabel_interval) p.relabel_interval_max = 16 * p.relabel_interval;
@@ -404,7 +405,7 @@ int engine_cut(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, std::vector<GridR
 }
 
 int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<GridResult>& res,
-                 jfc_stats& st) {
+                 jfc_stats& st, const GridDev* fast_grid) {
   jfc_params p = p_in;
   fill_defaults(p);
   cudaStream_t s = ctx->stream;
@@ -439,6 +440,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   // its sweeps: the relabel is then the bottleneck and is amortised.
   int interval = p.relabel_interval;
   bool graphs = false;
+  double fast_ms = 0.0;   // Fast-Cut iterations (event-timed: many small launches)
   unsigned long long last_pr = 0, last_gr = 0;
   {
     const DevCounters* c0 = (const DevCounters*)ctx->h_pin;
@@ -453,8 +455,23 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
     // relabel_interval x (even sweep, odd sweep), global relabel, active-tile
     // count: one host read-back per cycle
     int sw = 0;
-    rc = run_cycle(ctx, ts, p, interval, st.bfs_passes, active, &sw, &graphs);
-    if (rc) return rc;
+    if (p.pr_mode == 1 && fast_grid) {
+      // Fast-Cut comparison: `interval` line-sweep iterations, then the
+      // exact global relabel and convergence test
+      cudaEvent_t f0 = ev[2], f1 = ev[3];
+      JFC_CUDA(cudaEventRecord(f0, s));
+      for (int it = 0; it < interval; ++it) JFC_CUDA(launch_fast_iteration(*fast_grid, &ts.d_ctr->fast_moved, s));
+      JFC_CUDA(cudaEventRecord(f1, s));
+      rc = engine_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, nullptr);
+      if (rc) return rc;
+      const double fms = elapsed_ms(f0, f1);
+      fast_ms += fms;
+      last_pr -= (unsigned long long)(fms * 1e6);   // the cost rule below sees the sweeps' time
+      sw = 2 * interval;
+    } else {
+      rc = run_cycle(ctx, ts, p, interval, st.bfs_passes, active, &sw, &graphs);
+      if (rc) return rc;
+    }
     st.sweeps += sw;
     {
       const DevCounters* c1 = (const DevCounters*)ctx->h_pin;
@@ -502,7 +519,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   st.ms_gr_first = hv[3] * 1e-6;
   st.ms_gr_frontier = hv[4] * 1e-6;
   st.ms_global_relabel = st.ms_gr_first + st.ms_gr_frontier;
-  st.ms_push_relabel = hv[5] * 1e-6;
+  st.ms_push_relabel = hv[5] * 1e-6 + fast_ms;
   if (p.verbose >= 2)   // phase-clock split (non-zero in JFC_PHASE_CLOCK builds)
     fprintf(stderr, "{\"pr_cycles\": {\"stage\": %llu, \"local_relabel\": %llu, \"rounds\": %llu, \"exact_local\": %llu, "
                     "\"write_back\": %llu, \"grid_barrier\": %llu}}\n",

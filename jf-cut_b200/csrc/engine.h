@@ -54,8 +54,10 @@ struct GridResult {
 };
 
 // Solve every grid of `ts` to the exact max-flow (engine.cpp).
+// fast_grid: with p.pr_mode == 1, the single grid the Fast-Cut line sweeps run
+// on instead of the block-wise push-relabel phases.
 int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, std::vector<GridResult>& res,
-                 jfc_stats& st);
+                 jfc_stats& st, const GridDev* fast_grid = nullptr);
 // One BFS to its fixpoint in one persistent launch and its read-back: global
 // relabel (cut = false; active[g] = active tiles of grid g afterwards) or the
 // source-side cut (cut = true).  sweeps_done reports the sweeps of the

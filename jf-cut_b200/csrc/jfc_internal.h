@@ -52,6 +52,7 @@ struct DevCounters {
   int bfs_status;            // 1 converged, 2 pass budget exhausted
   int sweeps_done;           // sweeps run by the last push-relabel phase
   int pr_sweeps;             // sweep pairs of the next phase when launched with sweeps <= 0
+  int fast_moved;            // a Fast-Cut push moved flow (comparison mode)
   unsigned long long visits; // push-relabel tile visits
   unsigned long long bfs_visits;
   unsigned long long rounds; // push/relabel rounds summed over visits
@@ -94,6 +95,11 @@ cudaError_t launch_energy(int dims, int w, int h, int d, const int32_t* e, const
                           const uint8_t* lab, unsigned long long* out, cudaStream_t s);
 // (kernels_post.cu) p[i] &= keep over n bytes
 cudaError_t launch_and_bytes(uint8_t* p, long long n, uint8_t keep, cudaStream_t s);
+
+// (kernels_fast.cu) one Fast-Cut iteration on a single grid: relabel in two
+// parities, then line-segment pushes along each axis in two parities;
+// *moved (device) is raised when anything moved
+cudaError_t launch_fast_iteration(const GridDev& g, int* moved, cudaStream_t s);
 
 // Counts every kernel launch of the library (engine.cpp).
 void jfc_note_launch(int n = 1);

@@ -469,7 +469,7 @@ int jfc_solve(jfc_graph* G, jfc_stats* stats) {
   if (rc) return rc;
   std::vector<GridResult> res;
   jfc_stats st;
-  rc = engine_solve(G->ctx, G->ts, G->ctx->params, res, st);
+  rc = engine_solve(G->ctx, G->ts, G->ctx->params, res, st, &G->g);
   if (rc && rc != JFC_ERR_NOT_CONVERGED) return rc;
   G->flow = G->sink_total + res[0].neg_sum;
   G->source_nodes = res[0].labels;

@@ -453,6 +453,27 @@ def test_tag_post_process(ctx):
     g3.close()
 
 
+def test_fastcut_comparison_mode(ctx):
+    """The reference's Fast-Cut line sweeps (pr_mode 1) reach the same exact
+    max-flow and canonical cut as the block-wise solver."""
+    base = ctx.params()
+    try:
+        ctx.set_params(pr_mode=1, relabel_interval=2)
+        shape, e, caps, published, ref_object = load_fixture("flower")
+        g, st = solve_set(ctx, shape, e, caps)
+        assert g.flow() == published and st.status == 0
+        assert np.array_equal(g.labels().ravel(), ref_object)
+        g.close()
+        for k, shp in enumerate([(37, 53), (100, 300), (6, 20, 33), (13, 40, 70)]):
+            rng = np.random.default_rng(900 + k)
+            e, caps = random_grid(shp, rng, cap_max=60, density=0.4)
+            g, st = solve_set(ctx, shp, e, caps)
+            check_against_oracle(shp, e, caps, g.flow(), g.labels())
+            g.close()
+    finally:
+        ctx.set_params(pr_mode=0, relabel_interval=base.relabel_interval)
+
+
 def test_errors(ctx):
     img, seeds = jfcut.synth_gray_ellipse(64, 64, seed=1)
     g = jfcut.Graph(ctx, img.shape)

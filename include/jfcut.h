@@ -280,6 +280,28 @@ int jfc_graph_compute_tag(jfc_graph* g, const uint8_t* seeds, uint8_t* tag);
 int jfc_energy_device(int device, void* stream, int dims, int w, int h, int d, const int32_t* d_excess,
                       const int32_t* const* d_ncap, const uint8_t* d_labels, int64_t* data, int64_t* smooth);
 
+/* Stroke-to-seed mapping through a volume (graphcut_compute_visibility,
+ * graphcut_render_ray_casting.cl:275-346; compute only, no graphics): every
+ * pixel of the stroke mask (image_w x image_h, non-zero = stroke) casts a ray
+ * through the inverse view-projection (column-major, as the reference passes
+ * it) into the box [-box, box]; samples of the volume (trilinear, clamp to
+ * edge) are classified by the RGBA transfer function (tf_size entries,
+ * linear, after the intensity window) and composited front to back; each
+ * sample more opaque than alpha marks the 8 surrounding voxels with `label`
+ * in the dense seed array.  All arrays are device pointers; 3D volumes. */
+typedef struct jfc_view {
+  float inverse_mvp[16];
+  float box[3];                        /* volumeBoundingBox half extents */
+  int image_w, image_h;
+  int samples;                         /* sampleNumber (>= 3) */
+  float sample_ratio, sample_step_scale;
+  float window_width, window_level;
+  float alpha;
+} jfc_view;
+int jfc_stroke_to_seeds(int device, void* stream, const jfc_view* view, int w, int h, int d,
+                        const float* d_volume, const float* d_tf_rgba, int tf_size, const uint8_t* d_mask,
+                        uint8_t label, uint8_t* d_seeds);
+
 /* ---- the reference's data files (host only; no device work) ----
  * Dense arrays (w*h*d, x fastest) in the solver's channel order. */
 enum { JFC_FMT_UCHAR = 0, JFC_FMT_CHAR, JFC_FMT_USHORT, JFC_FMT_SHORT, JFC_FMT_UINT, JFC_FMT_INT, JFC_FMT_FLOAT };

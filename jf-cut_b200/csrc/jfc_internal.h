@@ -93,6 +93,9 @@ struct TileSet {
 // out[1] smooth (int64 sums, out zeroed by the caller)
 cudaError_t launch_energy(int dims, int w, int h, int d, const int32_t* e, const int32_t* const* caps,
                           const uint8_t* lab, unsigned long long* out, cudaStream_t s);
+// (kernels_post.cu) stroke-to-seed mapping through the volume (visibility)
+cudaError_t launch_stroke_seeds(const jfc_view& v, int w, int h, int d, const float* vol, const float* tf, int ntf,
+                                const uint8_t* mask, uint8_t label, uint8_t* seeds, cudaStream_t s);
 // (kernels_post.cu) p[i] &= keep over n bytes
 cudaError_t launch_and_bytes(uint8_t* p, long long n, uint8_t keep, cudaStream_t s);
 

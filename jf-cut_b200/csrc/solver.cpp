@@ -577,6 +577,20 @@ int jfc_graph_compute_tag(jfc_graph* G, const uint8_t* seeds, uint8_t* tag) {
   return JFC_OK;
 }
 
+int jfc_stroke_to_seeds(int device, void* stream, const jfc_view* view, int w, int h, int d,
+                        const float* d_volume, const float* d_tf_rgba, int tf_size, const uint8_t* d_mask,
+                        uint8_t label, uint8_t* d_seeds) {
+  if (!view || !d_volume || !d_tf_rgba || !d_mask || !d_seeds) return set_error(JFC_ERR_INVALID_ARG, "null argument");
+  if (w < 2 || h < 2 || d < 2 || tf_size < 1 || view->samples < 3 || view->image_w < 1 || view->image_h < 1 ||
+      !(view->box[0] > 0 && view->box[1] > 0 && view->box[2] > 0) || label > JFC_SEED_BG)
+    return set_error(JFC_ERR_INVALID_ARG, "bad volume, view or label");
+  JFC_CUDA(cudaSetDevice(device));
+  cudaStream_t s = (cudaStream_t)stream;
+  JFC_CUDA(launch_stroke_seeds(*view, w, h, d, d_volume, d_tf_rgba, tf_size, d_mask, label, d_seeds, s));
+  JFC_CUDA(cudaStreamSynchronize(s));
+  return JFC_OK;
+}
+
 int jfc_energy_device(int device, void* stream, int dims, int w, int h, int d, const int32_t* d_excess,
                       const int32_t* const* d_ncap, const uint8_t* d_labels, int64_t* data, int64_t* smooth) {
   if (!d_excess || !d_ncap || !d_labels || !data || !smooth) return set_error(JFC_ERR_INVALID_ARG, "null argument");

@@ -77,6 +77,14 @@ class VolumeInfo(ctypes.Structure):
                 ("intensity_min", ctypes.c_float), ("intensity_max", ctypes.c_float)]
 
 
+class View(ctypes.Structure):
+    """Ray-casting view of the stroke-to-seed mapping (jfc_view)."""
+    _fields_ = [("inverse_mvp", ctypes.c_float * 16), ("box", ctypes.c_float * 3), ("image_w", ctypes.c_int),
+                ("image_h", ctypes.c_int), ("samples", ctypes.c_int), ("sample_ratio", ctypes.c_float),
+                ("sample_step_scale", ctypes.c_float), ("window_width", ctypes.c_float),
+                ("window_level", ctypes.c_float), ("alpha", ctypes.c_float)]
+
+
 class MfiInfo(ctypes.Structure):
     _fields_ = [("dims", ctypes.c_int), ("conn", ctypes.c_int), ("w", ctypes.c_int), ("h", ctypes.c_int),
                 ("d", ctypes.c_int), ("maxflow", ctypes.c_int64), ("active_count", ctypes.c_int),
@@ -153,6 +161,8 @@ def _lib():
         L.jfc_server_cancel.argtypes = [VP, ctypes.c_int]
         L.jfc_server_get_stats.argtypes = [VP, ctypes.POINTER(ServerStats)]
         L.jfc_graph_compute_tag.argtypes = [VP, U8P, U8P]
+        L.jfc_stroke_to_seeds.argtypes = [ctypes.c_int, VP, ctypes.POINTER(View), ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, VP, VP, ctypes.c_int, VP, ctypes.c_uint8, VP]
         L.jfc_energy_device.argtypes = [ctypes.c_int, VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         VP, ctypes.POINTER(VP), VP, ctypes.POINTER(ctypes.c_int64),
                                         ctypes.POINTER(ctypes.c_int64)]
@@ -515,6 +525,14 @@ def energy_device(device, shape, d_excess, d_caps, d_labels, stream=0):
     _check(_lib().jfc_energy_device(int(device), VP(stream or None), dims, w, h, d, VP(d_excess), P, VP(d_labels),
                                     ctypes.byref(data), ctypes.byref(smooth)), "jfc_energy_device")
     return data.value, smooth.value
+
+
+def stroke_to_seeds(device, view, shape, d_volume, d_tf, tf_size, d_mask, label, d_seeds, stream=0):
+    """Mark the voxels a stroke sees through the volume (device pointers; shape (d, h, w))."""
+    d, h, w = (int(v) for v in shape)
+    _check(_lib().jfc_stroke_to_seeds(int(device), VP(stream or None), ctypes.byref(view), w, h, d, VP(d_volume),
+                                      VP(d_tf), int(tf_size), VP(d_mask), int(label), VP(d_seeds)),
+           "jfc_stroke_to_seeds")
 
 
 # ---------------------------------------------------------------- data files

@@ -474,6 +474,59 @@ def test_fastcut_comparison_mode(ctx):
         ctx.set_params(pr_mode=0, relabel_interval=base.relabel_interval)
 
 
+def _view_matrix():
+    """Column-major inverse view-projection: NDC (u, v, z) -> world, an
+    orthographic camera looking down -z, rotated a little about y and x."""
+    ca, sa, cb, sb = np.cos(0.3), np.sin(0.3), np.cos(0.2), np.sin(0.2)
+    ry = np.array([[ca, 0, sa, 0], [0, 1, 0, 0], [-sa, 0, ca, 0], [0, 0, 0, 1]])
+    rx = np.array([[1, 0, 0, 0], [0, cb, -sb, 0], [0, sb, cb, 0], [0, 0, 0, 1]])
+    ortho = np.array([[1.3, 0, 0, 0], [0, 1.3, 0, 0], [0, 0, -4.0, -1.0], [0, 0, 0, 1]])
+    mat = rx @ ry @ ortho                      # world = mat @ (u, v, z, 1)
+    return mat.T.ravel().astype(np.float32)    # column-major
+
+
+def test_stroke_to_seeds_matches_cpu_restatement(ctx):
+    """Visibility mapping of a stroke through a volume (float ray march):
+    device and CPU restatement agree on the marked voxels up to samples that
+    sit on the opacity threshold (tolerance: 1% of the marked set)."""
+    import torch
+    import visibility
+    d, h, w = 20, 28, 36
+    zz, yy, xx = np.mgrid[0:d, 0:h, 0:w].astype(np.float32)
+    vol = (np.exp(-(((xx - 18) / 9) ** 2 + ((yy - 14) / 7) ** 2 + ((zz - 10) / 5) ** 2))
+           + 0.4 * np.exp(-(((xx - 6) / 4) ** 2 + ((yy - 20) / 4) ** 2 + ((zz - 4) / 3) ** 2))).astype(np.float32)
+    vol = np.clip(vol, 0, 1).astype(np.float32)
+    n = 64
+    ramp = np.linspace(0, 1, n, dtype=np.float32)
+    tf = np.stack([ramp, 1 - ramp, ramp * 0.5, ramp ** 2], 1).astype(np.float32)
+    ih, iw = 24, 32
+    mask = np.zeros((ih, iw), np.uint8)
+    mask[4:20, 6:26] = 1
+    view = jfcut.View()
+    m = _view_matrix()
+    for i in range(16):
+        view.inverse_mvp[i] = float(m[i])
+    for i in range(3):
+        view.box[i] = 1.0
+    view.image_w, view.image_h, view.samples = iw, ih, 96
+    view.sample_ratio, view.sample_step_scale = 0.9, 2.0
+    view.window_width, view.window_level, view.alpha = 1.0, 0.5, 0.3
+    dv = torch.from_numpy(vol).cuda()
+    dt = torch.from_numpy(tf).cuda()
+    dm = torch.from_numpy(mask).cuda()
+    ds = torch.zeros(d * h * w, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    jfcut.stroke_to_seeds(0, view, (d, h, w), dv.data_ptr(), dt.data_ptr(), n, dm.data_ptr(), jfcut.SEED_FG,
+                          ds.data_ptr())
+    gpu = ds.cpu().numpy().reshape(d, h, w)
+    cpu = visibility.stroke_to_seeds(vol, tf, mask, m, [1.0, 1.0, 1.0], 96, 0.9, 2.0, 1.0, 0.5, 0.3,
+                                     jfcut.SEED_FG, np.zeros((d, h, w), np.uint8))
+    marked = (gpu > 0) | (cpu > 0)
+    assert marked.sum() > 50                                  # the stroke does see the object
+    assert ((gpu > 0) != (cpu > 0)).sum() <= max(1, marked.sum() // 100)
+    assert set(np.unique(gpu)) <= {0, jfcut.SEED_FG}
+
+
 def test_errors(ctx):
     img, seeds = jfcut.synth_gray_ellipse(64, 64, seed=1)
     g = jfcut.Graph(ctx, img.shape)

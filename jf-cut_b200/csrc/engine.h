@@ -24,6 +24,7 @@ struct DevModel {
   uint8_t* d_seeds = nullptr;
   int* d_lut_s = nullptr;        // t-link tables [JFC_TQ + 1]
   int* d_lut_t = nullptr;
+  int lut_lambda_t = -1;         // lambda_t the t-link tables hold (-1: none)
   size_t img_bytes = 0;
 };
 

@@ -144,8 +144,18 @@ cudaError_t launch_seed_stats(const GridDev& g, const void* d_img, int pixfmt, c
                               int* d_minmax /*[2][3][2]*/, unsigned long long* d_count /*[2]*/,
                               uint32_t* d_list_f, uint32_t* d_list_b, unsigned int* d_fill /*[2]*/,
                               bool fill, cudaStream_t s);
-cudaError_t launch_kmeans_assign(const uint32_t* d_list, unsigned int n, int channels, int k,
-                                 const int* mu, unsigned long long* d_acc /*[k*4]*/, cudaStream_t s);
+// k-means state of both seed classes, resident on the device across the
+// queued iterations (class 0 = foreground list first, class 1 after it).
+struct KmeansDev {
+  int mu[2][JFC_MAX_K * 3];            // centres, fixed point 1/16
+  int k[2];
+  int live[2];                         // class still moving
+  unsigned long long n[2];             // list lengths
+  unsigned long long acc[2][JFC_MAX_K * 4];   // per centre: channel sums, count
+  unsigned int done;                   // blocks finished in the current launch
+};
+cudaError_t launch_kmeans(const uint32_t* d_list, KmeansDev* d_km, int pixfmt, unsigned long long nmax,
+                          int iters, cudaStream_t s);
 cudaError_t launch_build_graph(const GridDev& g, const void* d_img, const uint8_t* d_seeds,
                                const BuildModelDev& m, const int* d_lut_xy, const int* d_lut_z,
                                const int* d_lut_s, const int* d_lut_t,

@@ -76,7 +76,7 @@ struct BuildScratch {
   unsigned long long count[2];
   int minmax[12];
   unsigned int fill[2];
-  unsigned long long acc[2][JFC_MAX_K * 4];
+  KmeansDev km;
 };
 
 // n-link table: w(t) = round(scale * exp(-D(t) / (2 sigma^2))) with D(t) = t
@@ -146,6 +146,37 @@ int build_core(jfc_graph* G, const void* img, int pixfmt, const uint8_t* seeds, 
   const double sigma2 = pairs ? (double)hbs.sum / (double)pairs : 0.0;
   const double scale_xy = (double)m.lambda_n;
   const double scale_z = (double)m.lambda_n * (double)m.z_weight_pct / 100.0;
+  // 2. seed lists
+  const unsigned long long nf = hbs.count[0], nb = hbs.count[1];
+  if (nf == 0 || nb == 0) { cleanup(); return set_error(JFC_ERR_NO_SEEDS, "no labels: a seed class is empty"); }
+  uint32_t* d_list = nullptr;
+  JFC_B(cudaMallocAsync((void**)&d_list, sizeof(uint32_t) * (nf + nb), s));
+  temps.push_back(d_list);
+  JFC_B(launch_seed_stats(G->g, M.d_img, pixfmt, M.d_seeds, d_bs->minmax, d_bs->count, d_list, d_list + nf,
+                          d_bs->fill, true, s));
+
+  // 3. k-means per class (fixed point 1/16, integer distances, order-free
+  // sums), all iterations queued on the device; centres start evenly spaced
+  // between the per-channel seed minimum and maximum
+  const int C = jfc_pix_channels(pixfmt);
+  KmeansDev& km = hbs.km;
+  std::memset(&km, 0, sizeof(km));
+  km.k[0] = std::min<int>(std::min(m.k_fg, JFC_MAX_K), (int)std::min<unsigned long long>(nf, JFC_MAX_K));
+  km.k[1] = std::min<int>(std::min(m.k_bg, JFC_MAX_K), (int)std::min<unsigned long long>(nb, JFC_MAX_K));
+  km.n[0] = nf;
+  km.n[1] = nb;
+  km.live[0] = km.live[1] = 1;
+  for (int cls = 0; cls < 2; ++cls)
+    for (int j = 0; j < km.k[cls]; ++j)
+      for (int c = 0; c < C; ++c) {
+        const long long mn = hbs.minmax[(cls * 3 + c) * 2], mx = hbs.minmax[(cls * 3 + c) * 2 + 1];
+        km.mu[cls][j * 3 + c] = (int)(16 * mn + (16 * (mx - mn) * (2 * j + 1)) / (2 * km.k[cls]));
+      }
+  JFC_B(cudaMemcpyAsync(&d_bs->km, &km, sizeof(km), cudaMemcpyHostToDevice, s));
+  JFC_B(launch_kmeans(d_list, &d_bs->km, pixfmt, std::max(nf, nb), m.kmeans_iters, s));
+
+  // 4. while the device iterates: n-link tables (data-dependent sigma) and,
+  // when lambda_t changed, the t-link tables over the quantised probability
   std::vector<int> lxy = nlink_table(pixfmt, scale_xy, sigma2);
   std::vector<int> lz = G->dims == 3 ? nlink_table(pixfmt, scale_z, sigma2) : std::vector<int>();
   int* d_lxy = nullptr;
@@ -158,63 +189,24 @@ int build_core(jfc_graph* G, const void* img, int pixfmt, const uint8_t* seeds, 
     temps.push_back(d_lz);
     JFC_B(cudaMemcpyAsync(d_lz, lz.data(), sizeof(int) * lz.size(), cudaMemcpyHostToDevice, s));
   }
-
-  // 2. seed lists
-  const unsigned long long nf = hbs.count[0], nb = hbs.count[1];
-  if (nf == 0 || nb == 0) { cleanup(); return set_error(JFC_ERR_NO_SEEDS, "no labels: a seed class is empty"); }
-  uint32_t* d_list = nullptr;
-  JFC_B(cudaMallocAsync((void**)&d_list, sizeof(uint32_t) * (nf + nb), s));
-  temps.push_back(d_list);
-  JFC_B(launch_seed_stats(G->g, M.d_img, pixfmt, M.d_seeds, d_bs->minmax, d_bs->count, d_list, d_list + nf,
-                          d_bs->fill, true, s));
-
-  // 3. k-means per class (fixed point 1/16, integer distances, order-free sums)
-  const int C = jfc_pix_channels(pixfmt);
-  int k[2] = {std::min<int>(std::min(m.k_fg, JFC_MAX_K), (int)std::min<unsigned long long>(nf, JFC_MAX_K)),
-              std::min<int>(std::min(m.k_bg, JFC_MAX_K), (int)std::min<unsigned long long>(nb, JFC_MAX_K))};
-  int mu[2][JFC_MAX_K * 3];
-  std::memset(mu, 0, sizeof(mu));
-  for (int cls = 0; cls < 2; ++cls)
-    for (int j = 0; j < k[cls]; ++j)
-      for (int c = 0; c < C; ++c) {
-        const long long mn = hbs.minmax[(cls * 3 + c) * 2], mx = hbs.minmax[(cls * 3 + c) * 2 + 1];
-        mu[cls][j * 3 + c] = (int)(16 * mn + (16 * (mx - mn) * (2 * j + 1)) / (2 * k[cls]));
-      }
-  bool live[2] = {true, true};
-  const unsigned long long cnt[2] = {nf, nb};
-  for (int it = 0; it < m.kmeans_iters && (live[0] || live[1]); ++it) {
-    JFC_B(cudaMemsetAsync(d_bs->acc, 0, sizeof(hbs.acc), s));
-    for (int cls = 0; cls < 2; ++cls)
-      if (live[cls])
-        JFC_B(launch_kmeans_assign(d_list + (cls ? nf : 0), (unsigned)cnt[cls], C, k[cls], mu[cls],
-                                   d_bs->acc[cls], s));
-    JFC_B(cudaMemcpyAsync(hbs.acc, d_bs->acc, sizeof(hbs.acc), cudaMemcpyDeviceToHost, s));
-    JFC_B(cudaStreamSynchronize(s));
-    for (int cls = 0; cls < 2; ++cls) {
-      if (!live[cls]) continue;
-      bool moved = false;
-      for (int j = 0; j < k[cls]; ++j) {
-        const long long c4 = (long long)hbs.acc[cls][j * 4 + 3];
-        if (c4 == 0) continue;
-        for (int c = 0; c < C; ++c) {
-          const int v = (int)((16 * (long long)hbs.acc[cls][j * 4 + c] + c4 / 2) / c4);
-          if (v != mu[cls][j * 3 + c]) { mu[cls][j * 3 + c] = v; moved = true; }
-        }
-      }
-      live[cls] = moved;
+  if (M.lut_lambda_t != m.lambda_t) {
+    std::vector<int> ls(JFC_TQ + 1), lt(JFC_TQ + 1);
+    for (int q = 0; q <= JFC_TQ; ++q) {
+      const double pb = ((double)q + 0.5) / (double)(JFC_TQ + 1);
+      const double pf = ((double)JFC_TQ + 0.5 - (double)q) / (double)(JFC_TQ + 1);
+      ls[q] = (int)std::floor((double)m.lambda_t * -std::log(pb) + 0.5);
+      lt[q] = (int)std::floor((double)m.lambda_t * -std::log(pf) + 0.5);
     }
+    M.lut_lambda_t = -1;
+    JFC_B(cudaMemcpyAsync(M.d_lut_s, ls.data(), sizeof(int) * ls.size(), cudaMemcpyHostToDevice, s));
+    JFC_B(cudaMemcpyAsync(M.d_lut_t, lt.data(), sizeof(int) * lt.size(), cudaMemcpyHostToDevice, s));
+    M.lut_lambda_t = m.lambda_t;
   }
+  JFC_B(cudaMemcpyAsync(km.mu, d_bs->km.mu, sizeof(km.mu), cudaMemcpyDeviceToHost, s));
+  JFC_B(cudaStreamSynchronize(s));
+  const int (&mu)[2][JFC_MAX_K * 3] = km.mu;
+  const int k[2] = {km.k[0], km.k[1]};
 
-  // 4. t-link tables over the quantised probability, then the graph pass
-  std::vector<int> ls(JFC_TQ + 1), lt(JFC_TQ + 1);
-  for (int q = 0; q <= JFC_TQ; ++q) {
-    const double pb = ((double)q + 0.5) / (double)(JFC_TQ + 1);
-    const double pf = ((double)JFC_TQ + 0.5 - (double)q) / (double)(JFC_TQ + 1);
-    ls[q] = (int)std::floor((double)m.lambda_t * -std::log(pb) + 0.5);
-    lt[q] = (int)std::floor((double)m.lambda_t * -std::log(pf) + 0.5);
-  }
-  JFC_B(cudaMemcpyAsync(M.d_lut_s, ls.data(), sizeof(int) * ls.size(), cudaMemcpyHostToDevice, s));
-  JFC_B(cudaMemcpyAsync(M.d_lut_t, lt.data(), sizeof(int) * lt.size(), cudaMemcpyHostToDevice, s));
   BuildModelDev bm{};
   bm.pixfmt = pixfmt; bm.channels = C; bm.kf = k[0]; bm.kb = k[1]; bm.seed_cap = m.seed_cap;
   std::memcpy(bm.mu_f, mu[0], sizeof(bm.mu_f));

@@ -74,15 +74,15 @@ enum { JFC_SEED_NONE = 0, JFC_SEED_FG = 1, JFC_SEED_BG = 2 };
 typedef struct jfc_params {
   int tile_rows;         /* 2D tiles are 32 x tile_rows: 8 or 16 (default 16); 3D tiles
                             see tile_depth */
-  int local_iters;       /* push/relabel rounds per tile visit (default 16) */
-  int relabel_interval;  /* sweep pairs between global relabels at the start (default 4) */
+  int local_iters;       /* push/relabel rounds per tile visit (default 12) */
+  int relabel_interval;  /* sweep pairs between global relabels at the start (default 3) */
   int max_sweeps;        /* budget of sweeps -> JFC_ERR_NOT_CONVERGED (default 1<<20) */
   int max_bfs_passes;    /* budget of tile passes per BFS (default 1<<20) */
   int use_graph;         /* 1: replay each relabel cycle (push-relabel phase + global
                             relabel + read-back) as one CUDA graph launch (default) */
   int verbose;           /* 1: one JSON line per global relabel on stderr */
   int relabel_interval_max; /* adaptive interval cap: the interval doubles while fewer
-                               than 1/256 of the tiles are active (default 16 x interval) */
+                               than 1/256 of the tiles are active (default max(64, 16 x interval)) */
   int tile_depth;        /* 3D tiles: 0 = automatic (32 x 4 x 2); 1, 2 or 4 = tiles of
                             32 x (tile_rows / tile_depth) x tile_depth (4 needs tile_rows 16) */
   int pr_mode;           /* 0: block-wise push-relabel (default); 1: the reference's Fast-Cut

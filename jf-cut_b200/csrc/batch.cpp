@@ -180,15 +180,15 @@ int jfc_batch_autotune(jfc_batch* b, jfc_params* chosen) {
   if (rc) { b->ctx->params = base; return rc; }
   rc = trial(best, best_ms);
   if (rc) { b->ctx->params = base; return rc; }
-  const int intervals[] = {2, 4, 8, 16};
-  const int iters[] = {8, 16, 32};
+  const int intervals[] = {2, 3, 4, 8, 16};
+  const int iters[] = {8, 12, 16, 32};
   const int rows[] = {8, 16};
   const int depths[] = {0, 1, 2, 4};   // 3D tile depth (0 = automatic 32x4x2)
   bool has3d = false;
   for (jfc_graph* g : b->graphs) has3d |= g->dims == 3;
   for (int axis = 0; axis < (has3d ? 4 : 3); ++axis) {
     const int* vals = axis == 0 ? intervals : axis == 1 ? iters : axis == 2 ? rows : depths;
-    const int nv = axis == 0 ? 4 : axis == 1 ? 3 : axis == 2 ? 2 : 4;
+    const int nv = axis == 0 ? 5 : axis == 1 ? 4 : axis == 2 ? 2 : 4;
     const jfc_params center = best;
     for (int i = 0; i < nv; ++i) {
       jfc_params p = center;

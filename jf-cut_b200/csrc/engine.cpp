@@ -59,9 +59,9 @@ void fill_defaults(jfc_params& p) {
   if (p.tile_depth == 4 && p.tile_rows == 8) p.tile_depth = 2;
   if (p.tile_depth != 1 && p.tile_depth != 2 && p.tile_depth != 4) p.tile_depth = 0;
   if (p.pr_mode != 1) p.pr_mode = 0;
-  if (p.local_iters <= 0) p.local_iters = 16;
-  if (p.relabel_interval <= 0) p.relabel_interval = 4;
-  if (p.relabel_interval_max < p.relabel_interval) p.relabel_interval_max = 16 * p.relabel_interval;
+  if (p.local_iters <= 0) p.local_iters = 12;
+  if (p.relabel_interval <= 0) p.relabel_interval = 3;
+  if (p.relabel_interval_max < p.relabel_interval) p.relabel_interval_max = std::max(64, 16 * p.relabel_interval);
   if (p.max_sweeps <= 0) p.max_sweeps = 1 << 20;
   if (p.max_bfs_passes <= 0) p.max_bfs_passes = 1 << 20;
 }

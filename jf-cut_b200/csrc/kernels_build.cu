@@ -3,8 +3,8 @@
 //
 // Reference: graphcut_compute_capacity_bk/_lazy (graphcut_compute_capacity.cl:21-254),
 // graphcut_kmeans (graphcut_kmeans.cl:21-159) with the host loop
-// QGCWidget::kmeans (QGCWidget.cpp:1997-2107), graphcut_compute_excessflow_lazy
-// (graphcut_compute_excessflow.cl:47-77, 109-139).
+// QGCWidget::kmeans (QGCWidget.cpp:1997-2107) moved onto the device,
+// graphcut_compute_excessflow_lazy (graphcut_compute_excessflow.cl:47-77, 109-139).
 // The reference evaluates exp / log in float on the device; here every
 // floating-point step happens once on the host in double into int32 lookup
 // tables (n-link weight per contrast index, t-link cost per quantised

@@ -242,6 +242,8 @@ void fail_lane(jfc_server* S, Lane& L, int rc) {
 int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
   jfc_ctx* ctx = S->solve_ctx;
   const jfc_params& p = S->params;
+  const Clock::time_point t_start = Clock::now();
+  Clock::time_point t_form = t_start, t_relabel = t_start;   // host-side phase ends (verbose)
   // 1. push-relabel phase over the current members
   bool ran_pr[2] = {false, false};
   for (int k = 0; k < 2; ++k) {
@@ -291,6 +293,7 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
   L.joining.clear();
   // 3. global relabel over the (re-formed) set
   for (int k = 0; k < 2; ++k) {
+    if (k == 0) t_form = Clock::now();
     if (L.mem[k].empty()) {
       L.active[k].clear();
       continue;
@@ -315,6 +318,7 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
     S->sessions.erase(s->sid);
   }
   L.freeing.clear();
+  t_relabel = Clock::now();
   // 4. converged grids: cut BFS on a tile set of those grids alone
   long long still = 0;
   for (int k = 0; k < 2; ++k) {
@@ -360,9 +364,14 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
   // the dense relabel dominate, so relabel less often
   const long long nt = (long long)L.ts[0].ntiles * (L.mem[0].empty() ? 0 : 1) +
                        (long long)L.ts[1].ntiles * (L.mem[1].empty() ? 0 : 1);
-  if (p.verbose)
-    fprintf(stderr, "{\"lane\": \"%s\", \"members\": %zu, \"active_tiles\": %lld, \"tiles\": %lld, \"interval\": %d}\n",
-            lane_id == 0 ? "interactive" : "bulk", L.mem[0].size() + L.mem[1].size(), still, nt, L.interval);
+  if (p.verbose) {
+    const Clock::time_point t_end = Clock::now();
+    auto ms = [](Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+    fprintf(stderr, "{\"lane\": \"%s\", \"members\": %zu, \"active_tiles\": %lld, \"tiles\": %lld, \"interval\": %d, "
+                    "\"ms_phase_membership\": %.3f, \"ms_form_relabel\": %.3f, \"ms_cut\": %.3f}\n",
+            lane_id == 0 ? "interactive" : "bulk", L.mem[0].size() + L.mem[1].size(), still, nt, L.interval,
+            ms(t_start, t_form), ms(t_form, t_relabel), ms(t_relabel, t_end));
+  }
   if (still > 0 && still * 256 < nt) L.interval = std::min(L.interval * 2, p.relabel_interval_max);
   else L.interval = p.relabel_interval;
   return JFC_OK;

@@ -85,9 +85,12 @@ typedef struct jfc_params {
                                than 1/256 of the tiles are active (default max(64, 16 x interval)) */
   int tile_depth;        /* 3D tiles: 0 = automatic (32 x 4 x 2); 1, 2 or 4 = tiles of
                             32 x (tile_rows / tile_depth) x tile_depth (4 needs tile_rows 16) */
-  int pr_mode;           /* 0: block-wise push-relabel (default); 1: the reference's Fast-Cut
-                            line sweeps (graphcut_push_relabel_fast.cl), for comparison; plain
-                            solves only, relabel_interval iterations between global relabels */
+  int pr_mode;           /* 0: block-wise push-relabel (default; with 2D 32 x 16 tiles the
+                            push-relabel visits run on 32 x 8 halves, the relabel and cut on
+                            whole tiles); 1: the reference's Fast-Cut line sweeps
+                            (graphcut_push_relabel_fast.cl), for comparison; plain solves only,
+                            relabel_interval iterations between global relabels; 2: block-wise
+                            on whole 32 x 16 tiles */
 } jfc_params;
 
 /* Capacity model (replaces computeCapacity / kmeans / computeExcessFlowLazy,

@@ -31,7 +31,8 @@ int rebuild(jfc_batch* b) {
   for (int k = 0; k < 2; ++k) {
     const int dims = k ? 3 : 2;
     const int td = b->ctx->params.tile_depth;
-    const int code = shape_code(dims, tr, td);
+    const bool split = pr_split_for(b->ctx->params, dims);
+    const int code = shape_code(dims, tr, td, split);
     if (!b->dirty && b->shape[k] == code) continue;
     std::vector<GridDev> v;
     for (jfc_graph* g : b->graphs)
@@ -39,7 +40,7 @@ int rebuild(jfc_batch* b) {
     tileset_free(b->ts[k]);
     b->shape[k] = -1;
     if (v.empty()) continue;
-    int rc = tileset_build(b->ts[k], dims, tr, td, v);
+    int rc = tileset_build(b->ts[k], dims, tr, td, v, nullptr, split);
     if (rc) return rc;
     b->shape[k] = code;
   }

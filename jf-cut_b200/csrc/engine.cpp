@@ -58,7 +58,7 @@ void fill_defaults(jfc_params& p) {
   // 3D tile depth: 0 = automatic (32 x 4 x 2 tiles); 4 needs tile_rows 16
   if (p.tile_depth == 4 && p.tile_rows == 8) p.tile_depth = 2;
   if (p.tile_depth != 1 && p.tile_depth != 2 && p.tile_depth != 4) p.tile_depth = 0;
-  if (p.pr_mode != 1) p.pr_mode = 0;
+  if (p.pr_mode != 1 && p.pr_mode != 2) p.pr_mode = 0;
   if (p.local_iters <= 0) p.local_iters = 12;
   if (p.relabel_interval <= 0) p.relabel_interval = 3;
   if (p.relabel_interval_max < p.relabel_interval) p.relabel_interval_max = std::max(64, 16 * p.relabel_interval);
@@ -72,9 +72,11 @@ double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
   return (double)ms;
 }
 
-int shape_code(int dims, int tile_rows, int tile_depth) {
-  return dims * 1000 + tile_rows * 10 + (dims == 3 ? tile_depth : 0);
+int shape_code(int dims, int tile_rows, int tile_depth, bool pr_split) {
+  return dims * 1000 + tile_rows * 10 + (dims == 3 ? tile_depth : 0) + (pr_split ? 100000 : 0);
 }
+
+bool pr_split_for(const jfc_params& p, int dims) { return dims == 2 && p.tile_rows == 16 && p.pr_mode != 2; }
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -92,7 +94,7 @@ static void tileset_carve(TileSet& ts, char* blk, size_t* total) {
   auto take = [&](size_t bytes) { const size_t o = off; off = align_up(off + bytes, 256); return o; };
   const size_t o_desc = take(sizeof(GridDev) * ng);
   const size_t o_info = take(sizeof(int4) * nt);
-  const size_t o_fpr = take(sizeof(int) * nt);
+  const size_t o_fpr = take(sizeof(int) * nt * 2);   // half-tile work items
   size_t o_qpr[2][2];
   for (int p = 0; p < 2; ++p)
     for (int b = 0; b < 2; ++b) o_qpr[p][b] = take(sizeof(int) * nt);
@@ -122,7 +124,7 @@ static void tileset_carve(TileSet& ts, char* blk, size_t* total) {
 }
 
 int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const std::vector<GridDev>& grids_in,
-                  cudaStream_t s) {
+                  cudaStream_t s, bool pr_split) {
   int TY, TZ;
   if (dims == 2) {
     TY = tile_rows; TZ = 1;
@@ -169,6 +171,7 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const st
   tileset_drop_graphs(ts);   // captured launches hold the old tile set by value
   ts.dims = dims;
   ts.TR = tile_rows; ts.TY = TY; ts.TZ = TZ;
+  ts.pr_split = pr_split && dims == 2 && TY == 16 ? 1 : 0;
   ts.ngrids = ngrids;
   ts.ntiles = ntiles;
   const size_t desc_bytes = sizeof(GridDev) * (size_t)ngrids, info_bytes = sizeof(int4) * (size_t)ntiles;

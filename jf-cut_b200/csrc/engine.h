@@ -72,11 +72,13 @@ int engine_cut(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, std::vector<GridR
 // tables are uploaded asynchronously from pinned staging (rewrite it only
 // after the next host sync on that stream) and a new block gets headroom.
 int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const std::vector<GridDev>& grids,
-                  cudaStream_t s = nullptr);
+                  cudaStream_t s = nullptr, bool pr_split = false);
 void tileset_free(TileSet& ts);
 // Drop the tile set's captured relabel-cycle graphs.
 void tileset_drop_graphs(TileSet& ts);
-int shape_code(int dims, int tile_rows, int tile_depth);
+int shape_code(int dims, int tile_rows, int tile_depth, bool pr_split);
+// 2D 32x16 tile sets run push-relabel on 32x8 halves unless pr_mode == 2
+bool pr_split_for(const jfc_params& p, int dims);
 
 int set_error(int code, const std::string& msg);
 int cuda_status(cudaError_t e, const char* where);

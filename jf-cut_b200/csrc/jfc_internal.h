@@ -68,12 +68,14 @@ struct DevCounters {
 struct TileSet {
   int dims = 2;
   int TR = 16, TY = 4, TZ = 4;       // tile shape (2D: 32xTR, 3D: 32xTYxTZ)
+  int pr_split = 0;                  // 2D 32x16 tiles: push-relabel runs on 32x8 halves
+                                     // (work item 2 * tile + half; relabel and cut on whole tiles)
   int ngrids = 0;
   int ntiles = 0;
   GridDev* d_desc = nullptr;         // [ngrids]
   int4* d_info = nullptr;            // [ntiles] {grid, tx, ty, tz}
   int nlist[2] = {0, 0};             // tiles of parity 0 / 1
-  int* d_flag_pr = nullptr;          // [ntiles] tile waits in a push-relabel queue
+  int* d_flag_pr = nullptr;          // [2 * ntiles] work item waits in a push-relabel queue
   int* d_q_pr[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [parity][buffer]
   int* d_flag_bfs[2] = {nullptr, nullptr};  // [buffer][ntiles] tile waits in a BFS frontier
   int* d_q_bfs[2] = {nullptr, nullptr};     // [buffer] BFS frontiers

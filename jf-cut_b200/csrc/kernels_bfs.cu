@@ -437,7 +437,17 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
     if (DIMS == 3 && z == 0) s.face[4] = 1;
     if (DIMS == 3 && z == TZ - 1) s.face[5] = 1;
   }
-  const bool act = __syncthreads_or(pos & (hf < JFC_INF));
+  // activity per 8-row half of a 2D 32x16 tile (bit 0 rows 0-7, bit 1 rows
+  // 8-15: the push-relabel work items of split tile sets), else bit 0
+  const bool live = pos & (hf < JFC_INF);
+  bool act_lo, act_hi = false;
+  if constexpr (DIMS == 2 && TY == 16) {
+    act_lo = __syncthreads_or(live && y < 8);
+    act_hi = __syncthreads_or(live && y >= 8);
+  } else {
+    act_lo = __syncthreads_or(live);
+  }
+  const bool act = act_lo || act_hi;
   if (t < 32) {
     const int txs = g.tiles_x, tys = g.tiles_y;
     bool want = false;
@@ -454,8 +464,8 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
     }
     jfc::warp_append(want, nb, Q.flags, Q.q, Q.qn);
     if (t == 0) {
-      const int old = (int)ts.d_act[tid];
-      ts.d_act[tid] = act ? 1 : 0;
+      const int old = ts.d_act[tid] != 0 ? 1 : 0;
+      ts.d_act[tid] = (uint8_t)((act_lo ? 1 : 0) | (act_hi ? 2 : 0));
       if (ti.x != cur_grid) {
         if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
         delta = 0;
@@ -579,7 +589,7 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
       if ((N[i] >> lane) & 1u) h[i] = d + 1;
     }
   }
-  unsigned rows_fin = 0, c0 = 0, c31 = 0, act = 0;
+  unsigned rows_fin = 0, c0 = 0, c31 = 0, act = 0, act_hi = 0;
 #pragma unroll
   for (int i = 0; i < R; ++i) {
     g.h[roff<TY>(a, i)] = h[i];
@@ -587,11 +597,14 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
     if (fin) rows_fin |= 1u << i;
     c0 |= fin & 1u;
     c31 |= fin >> 31;
-    act |= POS[i] & V[i];
+    // activity per 8-row half of a 2D 32x16 tile (push-relabel work items)
+    if (DIMS == 2 && TY == 16 && i >= 8) act_hi |= POS[i] & V[i];
+    else act |= POS[i] & V[i];
   }
   if (lane == 0) {
     const int old = 0;
-    ts.d_act[tid] = act ? 1 : 0;
+    ts.d_act[tid] = (uint8_t)((act ? 1 : 0) | (act_hi ? 2 : 0));
+    act |= act_hi;
     if (ti.x != cur_grid) {
       if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
       delta = 0;
@@ -737,7 +750,7 @@ __device__ __forceinline__ void relabel_frontier_warp(const TileSet& ts, int tid
   for (int i = 0; i < R; ++i) act |= ((posm >> i) & 1u) && hv[i] < JFC_INF;
   act = __any_sync(FULL, act);
   if (lane == 0) {
-    const int old = (int)ts.d_act[tid];
+    const int old = ts.d_act[tid] != 0 ? 1 : 0;
     ts.d_act[tid] = act ? 1 : 0;
     if (ti.x != cur_grid) {
       if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
@@ -747,6 +760,42 @@ __device__ __forceinline__ void relabel_frontier_warp(const TileSet& ts, int tid
     delta += (act ? 1 : 0) - old;
   }
   flag_neighbours<DIMS, TY, TZ>(g, a, tid, rows_changed, c0 != 0, c31 != 0, again, Q);
+}
+
+// Refill of the push-relabel queues (buffer 0 of each parity) from the
+// active-tile bits, warp-aggregated.  Split tile sets queue the active 8-row
+// halves as work items 2 * tile + half, half 0 with the tile's checkerboard
+// parity in the 32x8 tiling and half 1 with the other.
+__device__ __forceinline__ void refill_pr_queues(const TileSet& ts, DevCounters* ctr, int lane) {
+  for (;;) {
+    const unsigned c = jfc::warp_ticket(&ctr->ticket[0]);
+    const long long b = (long long)c * 32;
+    if (b >= ts.ntiles) break;
+    const long long t = b + lane;
+    bool w[2][2] = {{false, false}, {false, false}};   // [half][parity queue]
+    if (t < ts.ntiles) {
+      const unsigned bits = ts.d_act[t];
+      int par = 0;
+      if (bits) { const int4 ti = ts.d_info[t]; par = (ti.y + (ts.pr_split ? 2 * ti.z : ti.z) + ti.w) & 1; }
+      if (ts.pr_split) {
+        const bool a0 = (bits & 1u) != 0, a1 = (bits & 2u) != 0;
+        ts.d_flag_pr[2 * t] = a0 ? 1 : 0;
+        ts.d_flag_pr[2 * t + 1] = a1 ? 1 : 0;
+        w[0][par] = a0;
+        w[1][par ^ 1] = a1;
+      } else {
+        ts.d_flag_pr[t] = bits ? 1 : 0;
+        w[0][par] = bits != 0;
+      }
+    }
+    const int item0 = ts.pr_split ? (int)(2 * t) : (int)t;
+    jfc::warp_append(w[0][0], item0, nullptr, ts.d_q_pr[0][0], &ctr->qn_pr[0][0]);
+    jfc::warp_append(w[0][1], item0, nullptr, ts.d_q_pr[1][0], &ctr->qn_pr[1][0]);
+    if (ts.pr_split) {
+      jfc::warp_append(w[1][0], item0 + 1, nullptr, ts.d_q_pr[0][0], &ctr->qn_pr[0][0]);
+      jfc::warp_append(w[1][1], item0 + 1, nullptr, ts.d_q_pr[1][0], &ctr->qn_pr[1][0]);
+    }
+  }
 }
 
 // Global relabel, pass 0: every tile, one warp per tile (bit-parallel level
@@ -814,21 +863,7 @@ __global__ void __launch_bounds__(256) k_relabel_warp(TileSet ts, int max_passes
     ctr->cur_pr[0] = ctr->cur_pr[1] = 0;
   });
   if (ok) {
-    for (;;) {
-      const unsigned c = jfc::warp_ticket(&ctr->ticket[0]);
-      const long long b = (long long)c * 32;
-      if (b >= ts.ntiles) break;
-      const long long t = b + lane;
-      bool act = false;
-      int par = 0;
-      if (t < ts.ntiles) {
-        act = ts.d_act[t] != 0;
-        ts.d_flag_pr[t] = act ? 1 : 0;
-        if (act) { const int4 ti = ts.d_info[t]; par = (ti.y + ti.z + ti.w) & 1; }
-      }
-      jfc::warp_append(act && par == 0, (int)t, nullptr, ts.d_q_pr[0][0], &ctr->qn_pr[0][0]);
-      jfc::warp_append(act && par == 1, (int)t, nullptr, ts.d_q_pr[1][0], &ctr->qn_pr[1][0]);
-    }
+    refill_pr_queues(ts, ctr, lane);
     ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
   }
   // frontier visits are counted per warp (lane 0); pass 0 visited every tile
@@ -902,21 +937,7 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
     ctr->cur_pr[0] = ctr->cur_pr[1] = 0;
   });
   if (ok) {
-    for (;;) {
-      const unsigned c = jfc::warp_ticket(&ctr->ticket[0]);
-      const long long b = (long long)c * 32;
-      if (b >= ts.ntiles) break;
-      const long long t = b + lane;
-      bool act = false;
-      int par = 0;
-      if (t < ts.ntiles) {
-        act = ts.d_act[t] != 0;
-        ts.d_flag_pr[t] = act ? 1 : 0;
-        if (act) { const int4 ti = ts.d_info[t]; par = (ti.y + ti.z + ti.w) & 1; }
-      }
-      jfc::warp_append(act && par == 0, (int)t, nullptr, ts.d_q_pr[0][0], &ctr->qn_pr[0][0]);
-      jfc::warp_append(act && par == 1, (int)t, nullptr, ts.d_q_pr[1][0], &ctr->qn_pr[1][0]);
-    }
+    refill_pr_queues(ts, ctr, lane);
     ok = jfc::grid_sync(ctr, [&]() { ctr->ticket[0] = 0; });
   }
   // frontier visits are counted by warp 0 of each CTA; pass 0 visited every tile

@@ -58,17 +58,21 @@ __device__ __forceinline__ void halo_cell(int c, int& x, int& y, int& z, int& fa
   Tile<DIMS, TY, TZ>::halo_cell(c, x, y, z, face);
 }
 
-template <int DIMS, int TY, int TZ>
+// SPLIT: the work item `tid` is half `tid & 1` (rows 0-7 / 8-15) of the 2D
+// 32x16 tile `tid >> 1`, visited as a 32x8 tile; the halves keep their own
+// checkerboard parity, so the two halves of a tile never run at once.
+template <int DIMS, int TY, int TZ, bool SPLIT>
 __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_iters, bool local_relabel,
                                         PrSmem<DIMS, TY, TZ>& s, int* self_q, int* self_n, int* nbr_q, int* nbr_n) {
   using T = Tile<DIMS, TY, TZ>;
   const int t = threadIdx.x;
   const int x = t & 31, row = t >> 5, y = row % TY, z = row / TY;
-  const int4 ti = ts.d_info[tid];
+  const int tile = SPLIT ? tid >> 1 : tid, half = SPLIT ? tid & 1 : 0;
+  const int4 ti = ts.d_info[tile];
   const GridDev& g = ts.d_desc[ti.x];
   const int pitch = g.pitch;
   const long long slab = (long long)g.pitch * g.Hp;
-  const int x0 = ti.y * 32, y0 = ti.z * TY, z0 = ti.w * TZ;
+  const int x0 = ti.y * 32, y0 = SPLIT ? (2 * ti.z + half) * TY : ti.z * TY, z0 = ti.w * TZ;
   const long long tbase = (long long)x0 + (long long)y0 * pitch + (long long)z0 * slab;
   const long long n = tbase + x + (long long)y * pitch + (long long)z * slab;
   const int hi = T::hidx(x, y, z);
@@ -252,10 +256,10 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
     bool want = false;
     int nb = tid;
     switch (t) {
-      case 0: want = s.face[0]; nb = tid - 1; break;
-      case 1: want = s.face[1]; nb = tid + 1; break;
-      case 2: want = s.face[2]; nb = tid - txs; break;
-      case 3: want = s.face[3]; nb = tid + txs; break;
+      case 0: want = s.face[0]; nb = SPLIT ? tid - 2 : tid - 1; break;
+      case 1: want = s.face[1]; nb = SPLIT ? tid + 2 : tid + 1; break;
+      case 2: want = s.face[2]; nb = SPLIT ? (half ? tid - 1 : 2 * (tile - txs) + 1) : tid - txs; break;
+      case 3: want = s.face[3]; nb = SPLIT ? (half ? 2 * (tile + txs) : tid + 1) : tid + txs; break;
       case 4: want = DIMS == 3 && s.face[4]; nb = tid - txs * tys; break;
       case 5: want = DIMS == 3 && s.face[5]; nb = tid + txs * tys; break;
       default: break;
@@ -273,7 +277,7 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
 // by grid barriers.  Sweep s of parity p drains queue q_pr[p][cur_pr[p]] one
 // tile per CTA ticket; tiles still active go to q_pr[p][1-cur], neighbours
 // that received flow to the other parity's pending buffer.
-template <int DIMS, int TY, int TZ>
+template <int DIMS, int TY, int TZ, bool SPLIT>
 __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
     k_pr_phase(TileSet ts, int sweeps, int local_iters) {
   __shared__ PrSmem<DIMS, TY, TZ> sm;
@@ -301,8 +305,8 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
       // first sweep of a phase: nothing moved since the exact global relabel
       // (the halo tiles have the other parity), so the local relabel would
       // reproduce the heights it finds
-      rounds += pr_visit<DIMS, TY, TZ>(ts, tid, local_iters, s > 0, sm, ts.d_q_pr[p][b ^ 1], &ctr->qn_pr[p][b ^ 1],
-                                       ts.d_q_pr[p ^ 1][bo], &ctr->qn_pr[p ^ 1][bo]);
+      rounds += pr_visit<DIMS, TY, TZ, SPLIT>(ts, tid, local_iters, s > 0, sm, ts.d_q_pr[p][b ^ 1],
+                                              &ctr->qn_pr[p][b ^ 1], ts.d_q_pr[p ^ 1][bo], &ctr->qn_pr[p ^ 1][bo]);
       ++visits;
     }
     JFC_PCLK_DECL
@@ -324,21 +328,23 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
   }
 }
 
-template <int DIMS, int TY, int TZ>
+template <int DIMS, int TY, int TZ, bool SPLIT = false>
 cudaError_t launch_t(const TileSet& ts, int sweeps, int local_iters, cudaStream_t st) {
   constexpr int NT = Tile<DIMS, TY, TZ>::NT;
   static int blocks = 0;
-  if (!blocks) blocks = persistent_blocks((const void*)k_pr_phase<DIMS, TY, TZ>, NT, 0);
+  if (!blocks) blocks = persistent_blocks((const void*)k_pr_phase<DIMS, TY, TZ, SPLIT>, NT, 0);
   TileSet arg = ts;
   void* params[] = {(void*)&arg, (void*)&sweeps, (void*)&local_iters};
   jfc_note_launch();
-  return cudaLaunchCooperativeKernel((const void*)k_pr_phase<DIMS, TY, TZ>, dim3(blocks), dim3(NT), params, 0, st);
+  return cudaLaunchCooperativeKernel((const void*)k_pr_phase<DIMS, TY, TZ, SPLIT>, dim3(blocks), dim3(NT), params, 0,
+                                     st);
 }
 
 }  // namespace
 
 cudaError_t launch_pr_phase(const TileSet& ts, int sweeps, int local_iters, cudaStream_t s) {
   if (ts.dims == 2) {
+    if (ts.pr_split && ts.TR == 16) return launch_t<2, 8, 1, true>(ts, sweeps, local_iters, s);
     switch (ts.TR) {
       case 8: return launch_t<2, 8, 1>(ts, sweeps, local_iters, s);
       case 16: return launch_t<2, 16, 1>(ts, sweeps, local_iters, s);

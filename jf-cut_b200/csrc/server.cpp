@@ -301,7 +301,8 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
     if (changed[k]) {
       std::vector<GridDev> grids;
       for (Member& m : L.mem[k]) grids.push_back(m.s->G->g);
-      int rc = tileset_build(L.ts[k], k ? 3 : 2, p.tile_rows, p.tile_depth, grids, ctx->stream);
+      int rc = tileset_build(L.ts[k], k ? 3 : 2, p.tile_rows, p.tile_depth, grids, ctx->stream,
+                             pr_split_for(p, k ? 3 : 2));
       if (rc) return rc;
     }
     int passes = 0, sw = 0;

@@ -61,10 +61,11 @@ cudaError_t copy_plane(void* padded, const void* dense, size_t elem, const jfc_g
 }
 
 int ensure_tileset(jfc_graph* G) {
-  const int code = shape_code(G->dims, G->ctx->params.tile_rows, G->ctx->params.tile_depth);
+  const bool split = pr_split_for(G->ctx->params, G->dims);
+  const int code = shape_code(G->dims, G->ctx->params.tile_rows, G->ctx->params.tile_depth, split);
   if (G->ts_shape == code) return JFC_OK;
   std::vector<GridDev> v{G->g};
-  int rc = tileset_build(G->ts, G->dims, G->ctx->params.tile_rows, G->ctx->params.tile_depth, v);
+  int rc = tileset_build(G->ts, G->dims, G->ctx->params.tile_rows, G->ctx->params.tile_depth, v, nullptr, split);
   if (rc) return rc;
   G->ts_shape = code;
   return JFC_OK;

@@ -49,9 +49,12 @@ def test_golden_fixtures(ctx, name):
     assert bad == 0 and np.array_equal(lab2, lab)
 
 
-@pytest.mark.parametrize("tile_rows,local_iters,interval", [(8, 1, 1), (16, 4, 2), (8, 32, 16), (16, 16, 8)])
-def test_schedules_agree(ctx, tile_rows, local_iters, interval):
-    ctx.set_params(tile_rows=tile_rows, local_iters=local_iters, relabel_interval=interval)
+# pr_mode 0 with 32x16 tiles runs push-relabel on 32x8 halves of the relabel
+# tiles; pr_mode 2 on whole tiles
+@pytest.mark.parametrize("tile_rows,local_iters,interval,pr_mode",
+                         [(8, 1, 1, 0), (16, 4, 2, 0), (8, 32, 16, 0), (16, 16, 8, 0), (16, 12, 3, 2), (16, 1, 1, 2)])
+def test_schedules_agree(ctx, tile_rows, local_iters, interval, pr_mode):
+    ctx.set_params(tile_rows=tile_rows, local_iters=local_iters, relabel_interval=interval, pr_mode=pr_mode)
     try:
         shape, e, caps, published, _ = load_fixture("sponge")
         g, st = solve_set(ctx, shape, e, caps)
@@ -59,7 +62,7 @@ def test_schedules_agree(ctx, tile_rows, local_iters, interval):
         _, _, _, olab = oracle.maxflow(shape, e, caps)
         assert np.array_equal(g.labels().ravel(), olab)
     finally:
-        ctx.set_params(tile_rows=16, local_iters=16, relabel_interval=8)
+        ctx.set_params(tile_rows=16, local_iters=16, relabel_interval=8, pr_mode=0)
 
 
 def test_graph_replay_matches_direct_launches(ctx):

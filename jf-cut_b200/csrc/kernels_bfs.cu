@@ -425,7 +425,20 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
   }
   if (t < 6) s.face[t] = 0;
   __syncthreads();
-  const bool converged = jfc::relax_cta<DIMS, TY, TZ>(s.h, s.arc, 16);
+  // a tile is queued when a neighbour's boundary heights changed, which may
+  // not lower anything here: relax only when some residual arc (in the tile
+  // or into the halo) still offers a shorter distance
+  int m = JFC_INF;
+  if (arcs & jfc::A_XP) m = min(m, s.h[hi + 1]);
+  if (arcs & jfc::A_XM) m = min(m, s.h[hi - 1]);
+  if (arcs & jfc::A_YP) m = min(m, s.h[hi + T::SY]);
+  if (arcs & jfc::A_YM) m = min(m, s.h[hi - T::SY]);
+  if constexpr (DIMS == 3) {
+    if (arcs & jfc::A_ZP) m = min(m, s.h[hi + T::SZ]);
+    if (arcs & jfc::A_ZM) m = min(m, s.h[hi - T::SZ]);
+  }
+  const bool need = __syncthreads_or(m + 1 < hstart);
+  const bool converged = need ? jfc::relax_cta<DIMS, TY, TZ>(s.h, s.arc, 16) : true;
   const int hf = s.h[hi];
   const bool changed = hf != hstart;
   if (changed) {

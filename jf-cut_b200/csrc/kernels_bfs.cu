@@ -903,6 +903,37 @@ __global__ void __launch_bounds__(256) k_relabel_warp(TileSet ts, int max_passes
 // the push-relabel queues are refilled with every tile holding an active node
 // (the reference's graphcut_count_node + clogs scan + graphcut_scatter_node,
 // graphcut_count_block.cl:19-65, as one warp-aggregated append).
+// After the dense first pass every tile's heights are the exact in-tile
+// distances (halo unknown), so a tile can only fall through an arc leaving
+// it: one warp checks the tile's border nodes against the halo (2D) and
+// queues the tile for a full visit only when some residual arc u -> v out of
+// the tile has h(v) + 1 < h(u).
+template <int TY>
+__device__ __forceinline__ bool border_improvable(const TileSet& ts, int tid, int lane) {
+  const int4 ti = ts.d_info[tid];
+  const GridDev& g = ts.d_desc[ti.x];
+  const long long pitch = g.pitch;
+  const int x0 = ti.y * 32, y0 = ti.z * TY;
+  const long long base = (long long)x0 + (long long)y0 * pitch;
+  bool imp = false;
+  if (y0 > 0) {   // top row, arcs -y
+    const long long n = base + lane;
+    if ((g.label[n] & jfc::A_YM) && g.h[n - pitch] + 1 < g.h[n]) imp = true;
+  }
+  if (y0 + TY < g.Hp) {   // bottom row, arcs +y
+    const long long n = base + lane + (TY - 1) * pitch;
+    if ((g.label[n] & jfc::A_YP) && g.h[n + pitch] + 1 < g.h[n]) imp = true;
+  }
+  if (lane < TY && x0 > 0) {   // left column, arcs -x
+    const long long n = base + lane * pitch;
+    if ((g.label[n] & jfc::A_XM) && g.h[n - 1] + 1 < g.h[n]) imp = true;
+  } else if (lane >= 16 && lane < 16 + TY && x0 + 32 < pitch) {   // right column, arcs +x
+    const long long n = base + 31 + (lane - 16) * pitch;
+    if ((g.label[n] & jfc::A_XP) && g.h[n + 1] + 1 < g.h[n]) imp = true;
+  }
+  return __any_sync(jfc::FULL, imp);
+}
+
 template <int DIMS, int TY, int TZ>
 __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet ts, int max_passes) {
   __shared__ RlSmem<DIMS, TY, TZ> sm;
@@ -924,18 +955,31 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
     BfsQ Q{ts.d_flag_bfs[cb ^ 1], ts.d_q_bfs[cb ^ 1], &ctr->qn_bfs[cb ^ 1]};
     const int* queue = ts.d_q_bfs[cb];
     int* fcur = ts.d_flag_bfs[cb];
-    for (;;) {
-      if (threadIdx.x == 0) {
-        const unsigned k = atomicAdd(&ctr->ticket[cb], 1u);
-        sm.ntile = (int)k < n ? queue[k] : -1;
-        if ((int)k < n) fcur[sm.ntile] = 0;
+    if (DIMS == 2 && pass == 1) {
+      // the tiles the dense pass queued: a warp-level border check, full
+      // visits from pass 2 on for the tiles that can fall
+      for (;;) {
+        const unsigned k = jfc::warp_ticket(&ctr->ticket[cb]);
+        if ((int)k >= n) break;
+        const int tt = queue[k];
+        if (lane == 0) fcur[tt] = 0;
+        const bool imp = border_improvable<TY>(ts, tt, lane);
+        jfc::warp_append(imp && lane == 0, tt, Q.flags, Q.q, Q.qn);
       }
-      __syncthreads();
-      const int tt = sm.ntile;
-      __syncthreads();
-      if (tt < 0) break;
-      relabel_visit<DIMS, TY, TZ>(ts, tt, sm, Q, cur_grid, delta);
-      if (threadIdx.x < 32) ++visits;
+    } else {
+      for (;;) {
+        if (threadIdx.x == 0) {
+          const unsigned k = atomicAdd(&ctr->ticket[cb], 1u);
+          sm.ntile = (int)k < n ? queue[k] : -1;
+          if ((int)k < n) fcur[sm.ntile] = 0;
+        }
+        __syncthreads();
+        const int tt = sm.ntile;
+        __syncthreads();
+        if (tt < 0) break;
+        relabel_visit<DIMS, TY, TZ>(ts, tt, sm, Q, cur_grid, delta);
+        if (threadIdx.x < 32) ++visits;
+      }
     }
     ok = jfc::grid_sync(ctr, [&]() {
       ctr->ticket[cb] = 0;

@@ -581,8 +581,11 @@ def main():
     ms_step = ms / args.steps
     value = replica_throughput(n, world, args.steps, ms)
     e2e = replica_throughput(n, world, args.steps, ms_e2e)
+    # one push-relabel visit: a 32 x rows tile (32 x 8 halves of the 32 x 16
+    # relabel tiles unless pr_mode 2), 48 B per node + 12 B per halo cell
     tr = ctx.params().tile_rows
-    bytes_per_visit = 32 * tr * 48 + (2 * 32 + 2 * tr) * 12
+    rows = 8 if tr == 16 and ctx.params().pr_mode != 2 else tr
+    bytes_per_visit = 32 * rows * 48 + (2 * 32 + 2 * rows) * 12
     achieved = visits * bytes_per_visit / (ms_pr / 1000.0) / 1e9 if ms_pr > 0 else 0.0
     peak, peak_kind = peaks()
     pr_launches = int(agg["global_relabels"]) - args.steps    # one phase per relabel cycle

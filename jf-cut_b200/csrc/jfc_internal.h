@@ -61,6 +61,9 @@ struct DevCounters {
   unsigned long long ns_pr;           // push-relabel phases, device ns
   unsigned long long t_gr_start;      // device clock at the start of the last relabel
   unsigned long long prof[8];         // SM-cycle split of push-relabel visits (JFC_PHASE_CLOCK builds)
+  unsigned wl_head;          // 2D relabel worklist: tickets taken
+  unsigned wl_tail;          // 2D relabel worklist: ring positions reserved
+  int wl_out;                // 2D relabel worklist: items queued and not yet fully visited
 };
 
 // A set of grids tiled with one tile shape: the unit every launch works on

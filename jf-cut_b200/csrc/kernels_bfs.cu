@@ -36,6 +36,47 @@ struct BfsQ {
   int* qn;
 };
 
+// Worklist of the asynchronous 2D relabel: a ring of `cap` tile slots (-1 =
+// empty) with the queued flags of BfsQ, a tail counter and the count of
+// items queued and not yet fully visited (zero = the relaxation is done).
+struct RlRing {
+  int* ring;
+  unsigned cap;
+  unsigned* tail;
+  int* out;
+  int* err;
+};
+
+// Append the tiles offered by the lanes of a warp that win their queued
+// flag: count them as outstanding first (so the count never reaches zero
+// while one is on its way), then reserve ring positions and claim each slot
+// (free, or freed by its reader within a few polls; bounded: after ~2^26
+// polls the error flag is raised).  Returns false after an error.
+__device__ __forceinline__ bool ring_append(bool want, int tile, int* flags, const RlRing& W) {
+  bool won = false;
+  if (want) won = atomicExch(flags + tile, 1) == 0;
+  const unsigned m = __ballot_sync(jfc::FULL, won);
+  if (!m) return true;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  unsigned base = 0;
+  if (lane == leader) {
+    atomicAdd(W.out, __popc(m));
+    base = atomicAdd(W.tail, (unsigned)__popc(m));
+  }
+  base = __shfl_sync(jfc::FULL, base, leader);
+  bool ok = true;
+  if (won) {
+    int* slot = W.ring + (base + __popc(m & ((1u << lane) - 1u))) % W.cap;
+    __threadfence();
+    unsigned long long spins = 0;
+    while (atomicCAS(slot, -1, tile) != -1) {
+      if (++spins > (1ull << 26) || *(volatile int*)W.err) { atomicExch(W.err, 1); ok = false; break; }
+      __nanosleep(64);
+    }
+  }
+  return __all_sync(jfc::FULL, ok);
+}
+
 template <int DIMS>
 struct Dirs {
   static constexpr int XP = 0, YP = 1;
@@ -392,9 +433,11 @@ struct RlSmem {
 // heights and the halo, close the in-tile distances (relax_cta), write the
 // heights that fell, queue the neighbours whose halo fell and the tile itself
 // when its fixpoint was not reached.
+// W.ring non-null: the asynchronous worklist (neighbours go to the ring).
 template <int DIMS, int TY, int TZ>
 __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem<DIMS, TY, TZ>& s,
-                                              const BfsQ& Q, int& cur_grid, int& delta) {
+                                              const BfsQ& Q, int& cur_grid, int& delta,
+                                              const RlRing& W = RlRing{nullptr, 0, nullptr, nullptr, nullptr}) {
   using T = RTile<DIMS, TY, TZ>;
   using D = Dirs<DIMS>;
   const int t = threadIdx.x;
@@ -412,15 +455,20 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
   const unsigned arcs = ab & 63u;
   const bool pos = (ab & 128u) != 0;
   s.arc[t] = (uint8_t)arcs;
-  const int hstart = g.h[n];
+  // heights other CTAs write while the worklist runs are read from L2 (the
+  // SM's L1 may hold an older copy of the line)
+  const bool fresh = W.ring != nullptr;
+  const int hstart = fresh ? __ldcg(g.h + n) : g.h[n];
   s.h[hi] = hstart;
   for (int c = t; c < T::NHALO; c += T::NT) {
     int hx, hy, hz, f;
     T::halo_cell(c, hx, hy, hz, f);
     const int gx = x0 + hx, gy = y0 + hy, gz = z0 + hz;
     int v = JFC_INF;
-    if (gx >= 0 && gx < pitch && gy >= 0 && gy < g.Hp && gz >= 0 && gz < g.Dp)
-      v = g.h[(long long)gx + (long long)gy * pitch + (long long)gz * slab];
+    if (gx >= 0 && gx < pitch && gy >= 0 && gy < g.Hp && gz >= 0 && gz < g.Dp) {
+      const int* p = g.h + (long long)gx + (long long)gy * pitch + (long long)gz * slab;
+      v = fresh ? __ldcg(p) : *p;
+    }
     s.h[T::hidx(hx, hy, hz)] = v;
   }
   if (t < 6) s.face[t] = 0;
@@ -443,6 +491,7 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
   const bool changed = hf != hstart;
   if (changed) {
     g.h[n] = hf;
+    if (W.ring) __threadfence();   // visible before any neighbour is queued
     if (x == 0) s.face[0] = 1;
     if (x == 31) s.face[1] = 1;
     if (y == 0) s.face[2] = 1;
@@ -475,9 +524,10 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
       case 6: want = !converged; nb = tid; break;
       default: break;
     }
-    jfc::warp_append(want, nb, Q.flags, Q.q, Q.qn);
+    if (W.ring) ring_append(want, nb, Q.flags, W);
+    else jfc::warp_append(want, nb, Q.flags, Q.q, Q.qn);
     if (t == 0) {
-      const int old = ts.d_act[tid] != 0 ? 1 : 0;
+      const int old = (fresh ? __ldcg(ts.d_act + tid) : ts.d_act[tid]) != 0 ? 1 : 0;
       ts.d_act[tid] = (uint8_t)((act_lo ? 1 : 0) | (act_hi ? 2 : 0));
       if (ti.x != cur_grid) {
         if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
@@ -775,6 +825,10 @@ __device__ __forceinline__ void relabel_frontier_warp(const TileSet& ts, int tid
   flag_neighbours<DIMS, TY, TZ>(g, a, tid, rows_changed, c0 != 0, c31 != 0, again, Q);
 }
 
+#ifndef JFC_GR_ASYNC
+#define JFC_GR_ASYNC 1
+#endif
+
 // Refill of the push-relabel queues (buffer 0 of each parity) from the
 // active-tile bits, warp-aggregated.  Split tile sets queue the active 8-row
 // halves as work items 2 * tile + half, half 0 with the tile's checkerboard
@@ -943,6 +997,7 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
   int cur_grid = -1, delta = 0;
   bool ok = true;
   int pass = 1;
+  bool to_worklist = false;
   const unsigned long long t1 = jfc::global_ns();
   for (pass = 1; ok; ++pass) {
     const int cb = pass & 1;
@@ -955,6 +1010,7 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
     BfsQ Q{ts.d_flag_bfs[cb ^ 1], ts.d_q_bfs[cb ^ 1], &ctr->qn_bfs[cb ^ 1]};
     const int* queue = ts.d_q_bfs[cb];
     int* fcur = ts.d_flag_bfs[cb];
+    to_worklist = JFC_GR_ASYNC && DIMS == 2 && pass == 1;
     if (DIMS == 2 && pass == 1) {
       // the tiles the dense pass queued: a warp-level border check, full
       // visits from pass 2 on for the tiles that can fall
@@ -984,7 +1040,73 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
     ok = jfc::grid_sync(ctr, [&]() {
       ctr->ticket[cb] = 0;
       ctr->qn_bfs[cb] = 0;
+      if (to_worklist) {
+        ctr->wl_head = 0;
+        ctr->wl_tail = (unsigned)ctr->qn_bfs[cb ^ 1];
+        ctr->wl_out = ctr->qn_bfs[cb ^ 1];
+      }
     });
+    if (to_worklist) { ++pass; break; }
+  }
+  if (ok && to_worklist) {
+    // 2D passes 2..: an asynchronous worklist instead of barrier-separated
+    // passes.  A tile whose boundary fell queues its neighbours at once and
+    // any free CTA takes them, so a distance wave crosses one tile per visit
+    // instead of one tile per pass (the relaxation is monotone: any order
+    // reaches the same exact distances).  A per-tile lock keeps two visits of
+    // one tile apart; the work is done when no queued item is left.
+    const unsigned cap = (unsigned)ts.ntiles;
+    int* ring = ts.d_q_bfs[0];          // the border check queued into buffer 0
+    int* busy = ts.d_flag_bfs[1];       // free after the border check
+    const unsigned n0 = jfc::vload((const int*)&ctr->wl_tail);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cap; i += (long long)gridDim.x * blockDim.x) {
+      if (i >= n0) ring[i] = -1;
+      busy[i] = 0;
+    }
+    ok = jfc::grid_sync(ctr, [&]() {});
+    const RlRing W{ring, cap, &ctr->wl_tail, &ctr->wl_out, &ctr->error};
+    const BfsQ Q{ts.d_flag_bfs[0], nullptr, nullptr};
+    while (ok) {
+      if (threadIdx.x == 0) {
+        int tile = -1;
+        const unsigned k = atomicAdd(&ctr->wl_head, 1u);
+        int* slot = ring + k % cap;
+        unsigned long long spins = 0;
+        for (;;) {   // bounded: the item arrives, or the work is done, or an error
+          if (*(volatile int*)slot >= 0) {
+            const int v = atomicExch(slot, -1);
+            if (v >= 0) { tile = v; break; }
+          }
+          if (*(volatile int*)&ctr->wl_out == 0 || *(volatile int*)&ctr->error) break;
+          if (++spins > (1ull << 26)) { atomicExch(&ctr->error, 1); break; }
+          __nanosleep(32);
+        }
+        if (tile >= 0) {
+          spins = 0;
+          while (atomicCAS(busy + tile, 0, 1) != 0) {
+            if (++spins > (1ull << 26) || *(volatile int*)&ctr->error) { atomicExch(&ctr->error, 1); tile = -1; break; }
+            __nanosleep(32);
+          }
+        }
+        if (tile >= 0) {
+          __threadfence();
+          atomicExch(Q.flags + tile, 0);   // dequeued before its heights are read
+          __threadfence();
+        }
+        sm.ntile = tile;
+      }
+      __syncthreads();
+      const int tt = sm.ntile;
+      __syncthreads();
+      if (tt < 0) break;
+      relabel_visit<DIMS, TY, TZ>(ts, tt, sm, Q, cur_grid, delta, W);   // ends with a block barrier
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicExch(busy + tt, 0);
+        atomicSub(&ctr->wl_out, 1);
+      }
+      if (threadIdx.x < 32) ++visits;
+    }
   }
   if (threadIdx.x == 0 && delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
   // refill the push-relabel queues (buffer 0 of each parity) from the

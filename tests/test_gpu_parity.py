@@ -244,7 +244,9 @@ def test_warm_seed_edits(ctx):
 
 
 def test_seed_edit_duplicates_last_wins(ctx):
-    # (the final residual state of a solve is not unique: flows and cuts are)
+    # (the final residual state of a solve is not unique, and the adaptive
+    # relabel interval follows device clocks: flows and cuts are unique, and
+    # the change an edit makes to the excess is fixed by the seeds alone)
     img, seeds = jfcut.synth_rgb_ellipses(160, 120, seed=12)
     rng = np.random.default_rng(4)
     n = seeds.size
@@ -260,8 +262,9 @@ def test_seed_edit_duplicates_last_wins(ctx):
         g = jfcut.Graph(ctx, seeds.shape)
         g.build_from_image(img, seeds, jfcut.PIX_RGB8, MODEL5)
         g.solve()
+        e_solved = g.state()[0].copy()
         g.edit_seeds(a, b)
-        e_edit = g.state()[0].copy()      # residual excess right after the edit
+        e_edit = g.state()[0] - e_solved   # the edit's change of the excess
         g.solve()
         out.append((g.flow(), g.labels().copy(), e_edit))
         g.close()

@@ -422,6 +422,9 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   } ev_free{ev};
   JFC_CUDA(cudaEventRecord(ev[0], s));
   JFC_CUDA(launch_clear_counters(ts, s));
+#ifndef JFC_NO_PREPUSH
+  if (p.pr_mode != 1) JFC_CUDA(launch_prepush(ts, s));   // the Fast-Cut comparison stays as it was
+#endif
   std::vector<int> active;
   int rc;
 

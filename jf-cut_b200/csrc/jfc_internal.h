@@ -118,6 +118,8 @@ void jfc_note_launch(int n = 1);
 // reads the count from the control block (pr_sweeps), so one captured graph
 // serves every interval
 cudaError_t launch_pr_phase(const TileSet& ts, int sweeps, int local_iters, cudaStream_t s);
+// Local pre-push inside every tile before the first relabel of a solve.
+cudaError_t launch_prepush(const TileSet& ts, cudaStream_t s);
 // (kernels_bfs.cu) one BFS to its fixpoint in one persistent launch:
 // global relabel (cut = false; also refills the push-relabel queues) or the
 // source-side cut (cut = true)

@@ -340,7 +340,91 @@ cudaError_t launch_t(const TileSet& ts, int sweeps, int local_iters, cudaStream_
                                      st);
 }
 
+// Local pre-push before the first relabel of a solve, one CTA per tile, the
+// tile in shared memory: along one arc slot at a time, every node with excess
+// pushes to its in-tile neighbour across that slot when the neighbour is a
+// deficit, at most the arc's residual and the deficit.  Along one slot a node
+// either sends (e > 0) or receives (e < 0, from its one neighbour on the other
+// side), so each step is race-free; JFC_PREPUSH_ROUNDS rounds over all slots.
+// These are ordinary preflow pushes (the exact relabel that follows gives
+// valid heights), so the maximum flow and the canonical cut do not change;
+// most of the excess that meets a deficit a step or two away cancels here, in
+// one read and one write of the tile, instead of in push-relabel visits.
+#ifndef JFC_PREPUSH_ROUNDS
+#define JFC_PREPUSH_ROUNDS 2
+#endif
+template <int DIMS, int TY, int TZ>
+__global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT) k_prepush(TileSet ts) {
+  using T = Tile<DIMS, TY, TZ>;
+  __shared__ int se[T::NT];
+  __shared__ int sr[T::K][T::NT];
+  const int t = threadIdx.x;
+  const int x = t & 31, row = t >> 5, y = row % TY, z = row / TY;
+  const int4 ti = ts.d_info[blockIdx.x];
+  const GridDev& g = ts.d_desc[ti.x];
+  const long long pitch = g.pitch, slab = (long long)g.pitch * g.Hp;
+  const long long n = (long long)ti.y * 32 + x + ((long long)ti.z * TY + y) * pitch + ((long long)ti.w * TZ + z) * slab;
+  const int e0 = g.e[n];
+  int r0[T::K];
+#pragma unroll
+  for (int k = 0; k < T::K; ++k) r0[k] = g.r[k][n];
+  // nothing to do unless the tile holds both excess and a deficit
+  const bool pos = __syncthreads_or(e0 > 0);
+  const bool neg = __syncthreads_or(e0 < 0);
+  if (!pos || !neg) return;
+  se[t] = e0;
+#pragma unroll
+  for (int k = 0; k < T::K; ++k) sr[k][t] = r0[k];
+  __syncthreads();
+  for (int rnd = 0; rnd < JFC_PREPUSH_ROUNDS; ++rnd) {
+#pragma unroll
+    for (int k = 0; k < T::K; ++k) {
+      const bool inside = k == T::XP ? x < 31 : k == T::XM ? x > 0 : k == T::YP ? y < TY - 1
+                        : k == T::YM ? y > 0 : k == T::ZP ? z < TZ - 1 : z > 0;
+      const int off = k == T::XP ? 1 : k == T::XM ? -1 : k == T::YP ? 32 : k == T::YM ? -32
+                    : k == T::ZP ? 32 * TY : -32 * TY;
+      const int e = se[t];
+      if (inside && e > 0) {
+        const int r = sr[k][t], ev = se[t + off];
+        if (r > 0 && ev < 0) {
+          const int d = min(min(e, r), -ev);
+          se[t] = e - d;
+          sr[k][t] = r - d;
+          se[t + off] = ev + d;
+          sr[T::K - 1 - k][t + off] += d;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  const int e1 = se[t];
+  if (e1 != e0) g.e[n] = e1;
+#pragma unroll
+  for (int k = 0; k < T::K; ++k) {
+    const int v = sr[k][t];
+    if (v != r0[k]) g.r[k][n] = v;
+  }
+}
+
+template <int DIMS, int TY, int TZ>
+cudaError_t prepush_t(const TileSet& ts, cudaStream_t st) {
+  jfc_note_launch();
+  k_prepush<DIMS, TY, TZ><<<(unsigned)ts.ntiles, Tile<DIMS, TY, TZ>::NT, 0, st>>>(ts);
+  return cudaGetLastError();
+}
+
 }  // namespace
+
+cudaError_t launch_prepush(const TileSet& ts, cudaStream_t s) {
+  if (ts.ntiles <= 0) return cudaSuccess;
+  if (ts.dims == 2) return ts.TR == 8 ? prepush_t<2, 8, 1>(ts, s) : prepush_t<2, 16, 1>(ts, s);
+  if (ts.TY == 4 && ts.TZ == 4) return prepush_t<3, 4, 4>(ts, s);
+  if (ts.TY == 4 && ts.TZ == 2) return prepush_t<3, 4, 2>(ts, s);
+  if (ts.TY == 16 && ts.TZ == 1) return prepush_t<3, 16, 1>(ts, s);
+  if (ts.TY == 8 && ts.TZ == 2) return prepush_t<3, 8, 2>(ts, s);
+  if (ts.TY == 8 && ts.TZ == 1) return prepush_t<3, 8, 1>(ts, s);
+  return cudaErrorInvalidValue;
+}
 
 cudaError_t launch_pr_phase(const TileSet& ts, int sweeps, int local_iters, cudaStream_t s) {
   if (ts.dims == 2) {

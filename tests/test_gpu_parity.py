@@ -126,10 +126,13 @@ def test_3d_tile_shapes(ctx, tile_rows, tile_depth):
 
 
 @pytest.mark.parametrize("shape,tile_rows,tile_depth", [((64, 96), 16, 4), ((33, 65), 8, 2), ((100, 1000), 16, 4),
+                                                      ((700, 1900), 16, 4), ((700, 1900), 8, 2),
                                                       ((8, 33, 31), 16, 4), ((13, 40, 70), 8, 2), ((9, 21, 40), 16, 1)])
 def test_final_heights_are_exact_distances(ctx, shape, tile_rows, tile_depth):
     """The last global relabel of a solve leaves the exact residual BFS
-    distance to the deficits in every node (INF where none is reachable)."""
+    distance to the deficits in every node (INF where none is reachable).
+    The 700 x 1900 grids keep hundreds of CTAs busy at once on the 2D
+    relabel worklist, so concurrent visits of neighbouring tiles happen."""
     base = ctx.params()
     try:
         ctx.set_params(tile_rows=tile_rows, tile_depth=tile_depth)

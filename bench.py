@@ -598,7 +598,8 @@ def main():
                                    "(build + solve + labels per step)" % (w, h),
                        "nodes": n, "global_batch": world, "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (state %.1f GB)" % (jfcut.lib().jfc_graph_bytes(2, w, h, 1) / 1e9),
-                       "params": {k: getattr(ctx.params(), k) for k in ("tile_rows", "local_iters", "relabel_interval")},
+                       "params": {"tile_rows": ctx.params().tile_rows, "local_iters": ctx.params().local_iters,
+                                  "relabel_interval": ctx.params().relabel_interval or "auto (2 for 2D grids)"},
                        "flow": flow_ref, "sweeps_per_step": sweeps / args.steps,
                        "solve_breakdown_per_step": {k: v / args.steps for k, v in agg.items()},
                        "pr_tile_visits_per_step": visits / args.steps},

@@ -75,7 +75,8 @@ typedef struct jfc_params {
   int tile_rows;         /* 2D tiles are 32 x tile_rows: 8 or 16 (default 16); 3D tiles
                             see tile_depth */
   int local_iters;       /* push/relabel rounds per tile visit (default 12) */
-  int relabel_interval;  /* sweep pairs between global relabels at the start (default 3) */
+  int relabel_interval;  /* sweep pairs between global relabels at the start (default 0 =
+                            automatic: 2 for 2D grids, 3 for 3D grids) */
   int max_sweeps;        /* budget of sweeps -> JFC_ERR_NOT_CONVERGED (default 1<<20) */
   int max_bfs_passes;    /* budget of tile passes per BFS (default 1<<20) */
   int use_graph;         /* 1: replay each relabel cycle (push-relabel phase + global

@@ -60,8 +60,9 @@ void fill_defaults(jfc_params& p) {
   if (p.tile_depth != 1 && p.tile_depth != 2 && p.tile_depth != 4) p.tile_depth = 0;
   if (p.pr_mode != 1 && p.pr_mode != 2) p.pr_mode = 0;
   if (p.local_iters <= 0) p.local_iters = 12;
-  if (p.relabel_interval <= 0) p.relabel_interval = 3;
-  if (p.relabel_interval_max < p.relabel_interval) p.relabel_interval_max = std::max(64, 16 * p.relabel_interval);
+  if (p.relabel_interval < 0) p.relabel_interval = 0;   // 0: automatic per dimensionality
+  if (p.relabel_interval_max <= 0 || p.relabel_interval_max < p.relabel_interval)
+    p.relabel_interval_max = std::max(64, 16 * p.relabel_interval);
   if (p.max_sweeps <= 0) p.max_sweeps = 1 << 20;
   if (p.max_bfs_passes <= 0) p.max_bfs_passes = 1 << 20;
 }
@@ -444,7 +445,8 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   //  The interval also doubles while the last relabel cost more than twice
   // the push-relabel phase before it (device clocks) and that phase used all
   // its sweeps: the relabel is then the bottleneck and is amortised.
-  int interval = p.relabel_interval;
+  const int interval0 = interval_for(p, ts.dims);
+  int interval = interval0;
   bool graphs = false;
   double fast_ms = 0.0;   // Fast-Cut iterations (event-timed: many small launches)
   unsigned long long last_pr = 0, last_gr = 0;
@@ -487,7 +489,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
       const bool sliver = total() * 256 < (long long)ts.ntiles;
       const bool relabel_bound = gr > 2 * pr && sw >= 2 * interval;
       if (sliver || relabel_bound) interval = std::min(interval * 2, p.relabel_interval_max);
-      else interval = p.relabel_interval;
+      else interval = interval0;
     }
     ++st.global_relabels;
     if (p.verbose) {

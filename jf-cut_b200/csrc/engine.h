@@ -79,6 +79,12 @@ void tileset_drop_graphs(TileSet& ts);
 int shape_code(int dims, int tile_rows, int tile_depth, bool pr_split);
 // 2D 32x16 tile sets run push-relabel on 32x8 halves unless pr_mode == 2
 bool pr_split_for(const jfc_params& p, int dims);
+// Sweep pairs between global relabels: relabel_interval, or when it is 0 the
+// measured best per dimensionality (2D: relabels are cheap next to the
+// push-relabel sweeps; 3D: the relabel dominates and runs less often).
+inline int interval_for(const jfc_params& p, int dims) {
+  return p.relabel_interval > 0 ? p.relabel_interval : (dims == 2 ? 2 : 3);
+}
 
 int set_error(int code, const std::string& msg);
 int cuda_status(cudaError_t e, const char* where);

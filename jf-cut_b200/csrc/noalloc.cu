@@ -219,7 +219,7 @@ extern "C" int jfc_solve_grid2d_noalloc(int device, void* stream, const jfc_para
   while (active > 0) {
     if (sweeps >= p.max_sweeps) return set_error(JFC_ERR_NOT_CONVERGED, "sweep budget exhausted");
     JFC_CUDA(cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s));
-    JFC_CUDA(launch_pr_phase(ts, p.relabel_interval, p.local_iters, s));
+    JFC_CUDA(launch_pr_phase(ts, interval_for(p, 2), p.local_iters, s));
     rc = na_bfs(ts, p, false, s, &active, nullptr);
     if (rc) return rc;
     int sw = 0;

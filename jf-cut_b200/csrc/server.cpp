@@ -374,7 +374,7 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
             ms(t_start, t_form), ms(t_form, t_relabel), ms(t_relabel, t_end));
   }
   if (still > 0 && still * 256 < nt) L.interval = std::min(L.interval * 2, p.relabel_interval_max);
-  else L.interval = p.relabel_interval;
+  else L.interval = interval_for(p, 2);
   return JFC_OK;
 }
 
@@ -382,7 +382,7 @@ void solver_loop(jfc_server* S) {
   cudaSetDevice(S->device);
   const jfc_params& p = S->params;
   Lane lanes[2];                    // [0] interactive (warm edits), [1] bulk (cold)
-  lanes[0].interval = lanes[1].interval = p.relabel_interval;
+  lanes[0].interval = lanes[1].interval = interval_for(p, 2);
   constexpr int kInteractiveCycles = 16;   // interactive cycles per bulk cycle, at most
   for (;;) {
     // admission: requests waiting for a slot join their lane at its next relabel

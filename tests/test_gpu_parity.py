@@ -344,7 +344,7 @@ def test_batch_autotune_restores_and_matches(ctx):
     base = ctx.params()
     try:
         p = b.autotune()
-        assert p.tile_rows in (8, 16) and p.local_iters in (8, 12, 16, 32) and p.relabel_interval in (2, 3, 4, 8, 16)
+        assert p.tile_rows in (8, 16) and p.local_iters in (8, 12, 16, 32) and p.relabel_interval in (0, 2, 3, 4, 8, 16)
         # the graphs are back in their built state: solving now gives the plain results
         st = b.solve()
         assert all(s.status == 0 for s in st)

@@ -10,7 +10,9 @@
 // B200 design:
 //  * one CTA per tile of 32 x TY (x TZ) nodes, one thread per node, one warp per
 //    tile row (128-byte coalesced row loads / stores); excess, heights (with
-//    the halo) and residual arcs live in shared memory for the visit;
+//    the halo) and residual arcs live in shared memory for the visit.  With 2D
+//    32 x 16 relabel tiles the visits work on their 32 x 8 halves (SPLIT),
+//    which keep a checkerboard parity of their own;
 //  * a round = one relabel step and one push step for all nodes at once
 //    (two block barriers per round):
 //    under a fixed height vector two neighbours never push to each other, so a

@@ -9,10 +9,13 @@
 // (graphcut_bfs_block.cl).  Here the relaxation is monotone (heights only fall
 // from INF), so tiles need no parity and no order: a persistent cooperative
 // kernel runs a first pass over every tile (fused initialisation, one warp
-// per tile, bit-parallel level BFS) and then frontier passes (a tile whose
-// boundary fell queues its neighbours, grid barrier between passes) in which
-// one CTA per tile closes the in-tile distances with warp min-plus scans
-// along rows and columns.  Each visit records whether the tile holds an
+// per tile, bit-parallel level BFS) and then the frontier (a tile whose
+// boundary fell queues its neighbours).  In 2D the frontier starts with a
+// one-warp border check of the tiles the first pass queued and continues as
+// an asynchronous worklist: one CTA per queued tile closes the in-tile
+// distances with warp min-plus scans along rows and columns.  In 3D it runs in
+// passes separated by grid barriers, one warp per queued tile (level BFS
+// seeded by the halo heights).  Each visit records whether the tile holds an
 // active node (e > 0, h < INF): the device-side active-tile count
 // (graphcut_count_node, graphcut_count_block.cl:19-47) that decides
 // convergence, and the queue of tiles the next push-relabel phase visits.

@@ -72,7 +72,7 @@ enum { JFC_SEED_NONE = 0, JFC_SEED_FG = 1, JFC_SEED_BG = 2 };
  * cutIterations, totalIterations: QGCPanel.ui:1494-1658) and the tile
  * constants (QGCSetting.cpp:28-29).  Zero fields take defaults. */
 typedef struct jfc_params {
-  int tile_rows;         /* 2D tiles are 32 x tile_rows: 8 or 16 (default 16); 3D tiles
+  int tile_rows;         /* 2D tiles are 32 x tile_rows: 8 (default) or 16; 3D tiles
                             see tile_depth */
   int local_iters;       /* push/relabel rounds per tile visit (default 12) */
   int relabel_interval;  /* sweep pairs between global relabels at the start (default 0 =

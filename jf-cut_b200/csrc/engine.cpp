@@ -54,7 +54,9 @@ int cuda_status(cudaError_t e, const char* where) {
 extern "C" const char* jfc_last_error(void) { return g_err.c_str(); }
 
 void fill_defaults(jfc_params& p) {
-  if (p.tile_rows != 8 && p.tile_rows != 16) p.tile_rows = 16;
+  // 2D tiles 32 x 8 by default: with the relabel worklist the small tiles no
+  // longer cost relabel passes, and their visits are the shortest
+  if (p.tile_rows != 8 && p.tile_rows != 16) p.tile_rows = 8;
   // 3D tile depth: 0 = automatic (32 x 4 x 2 tiles); 4 needs tile_rows 16
   if (p.tile_depth == 4 && p.tile_rows == 8) p.tile_depth = 2;
   if (p.tile_depth != 1 && p.tile_depth != 2 && p.tile_depth != 4) p.tile_depth = 0;

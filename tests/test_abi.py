@@ -49,7 +49,10 @@ def test_strerror_and_defaults():
     assert L.jfc_strerror(0) == b"ok"
     assert b"no labels" in L.jfc_strerror(2)
     p = jfcut.default_params()
-    assert p.tile_rows in (8, 16) and p.local_iters > 0 and p.relabel_interval >= 0   # 0: automatic
+    # the measured defaults: 32x8 tiles, 12 rounds per visit, automatic relabel
+    # interval (2D every 2 sweep pairs, 3D every 3), interval cap 64, graphs on
+    assert (p.tile_rows, p.local_iters, p.relabel_interval, p.relabel_interval_max) == (8, 12, 0, 64)
+    assert p.use_graph == 1 and p.pr_mode == 0 and p.tile_depth == 0
     m = jfcut.default_model()
     assert m.lambda_n == 100 and m.lambda_t == 10 and m.seed_cap == 1000000
 

@@ -36,8 +36,8 @@ METRIC = "Mnodes/s to exact min-cut (plain, 2D 4-conn 15000x10000 RGB)"
 
 
 def pr_traffic_per_launch():
-    """DRAM bytes per push-relabel phase launch from the committed ncu capture
-    of this workload (profiles/k_pr_phase_traffic_15000x10000.md), or None."""
+    """DRAM bytes per push-relabel phase launch from the committed summary of
+    the ncu capture of this workload (under profiles/), or None."""
     try:
         with open(os.path.join(ROOT, "profiles", "k_pr_phase_traffic_15000x10000.md")) as f:
             for line in f:

@@ -871,8 +871,11 @@ __device__ __forceinline__ void refill_pr_queues(const TileSet& ts, DevCounters*
 // Global relabel, pass 0: every tile, one warp per tile (bit-parallel level
 // BFS from the deficits, fused initialisation).  A plain launch: its many
 // registers do not limit the occupancy of the frontier kernel.
+// (32 x 8 2D tiles fit in 64 registers without spills: 4 CTAs per SM keep
+// twice the loads in flight of the 2-CTA bound the larger tiles need)
 template <int DIMS, int TY, int TZ>
-__global__ void __launch_bounds__(256, (DIMS == 3 && TY * TZ > 8) ? 1 : 2) k_relabel_first(TileSet ts) {
+__global__ void __launch_bounds__(256, (DIMS == 3 && TY * TZ > 8) ? 1 : (DIMS == 2 && TY == 8) ? 4 : 2)
+    k_relabel_first(TileSet ts) {
   DevCounters* ctr = ts.d_ctr;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctr->t_gr_start = jfc::global_ns();
   const int lane = threadIdx.x & 31;

@@ -28,6 +28,10 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "jf-cut_b200"))
+# seeded input generators (oracle/synthetic.cpp): both arms build their graph
+# from the same bytes; they run before any timed region
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import synthetic  # noqa: E402
 
 W_FULL, H_FULL = 15000, 10000
 SEED = 20240601
@@ -109,71 +113,89 @@ class ClockSampler:
 
 
 def make_workload(w, h, seed):
-    import jfcut
-    return jfcut.synth_rgb_ellipses(w, h, seed=seed, n_ellipses=20, noise_sigma=15, stroke_permille_x10=50)
+    return synthetic.rgb_ellipses(w, h, seed=seed, n_ellipses=20, noise_sigma=15, stroke_permille_x10=50)
 
 
-def reference_sample(budget_s=20.0, side=(2048, 1536)):
-    """Bounded sample of the same workload for the CPU solvers: one image of
-    `side` generated like the full one."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+def workload_name(w, h):
+    return ("plain: 2D 4-conn %dx%d RGB, 20 ellipses, N(0,15), 0.5%% strokes, 5-means "
+            "(build + solve + labels per step)" % (w, h))
+
+
+def cpu_graph(w, h, seed):
+    """The workload's graph built on the host by the CPU restatement of the
+    capacity build (the GPU build equals it bit for bit: the parity tests):
+    (oracle module, shape, e, caps, sum ct)."""
     import oracle
-    w, h = side
-    img, seeds = make_workload(w, h, SEED)
+    img, seeds = make_workload(w, h, seed)
     e, caps, sink = oracle.build_graph(img, seeds, 1, MODEL)
-    return oracle, (h, w), e, caps
+    return oracle, (h, w), e, caps, sink
+
+
+def full_flow(e0, folded, sink):
+    """Max-flow of the image graph from a solver's folded flow on the
+    net-excess graph (terminal arcs cs = max(e,0), ct = max(-e,0)):
+    sum ct + folded - sum max(-e, 0)."""
+    return int(sink) + int(folded) - int(np.maximum(-e0.astype(np.int64), 0).sum())
 
 
 def run_reference(args):
-    """Reference arm: the reference's own CPU solver (GridCut 1.1 multi-threaded,
-    built from the reference sources) on the host cores, bounded sample."""
+    """Reference arm: the reference's own CPU solver, GridCut 1.1
+    multi-threaded (benchmark/GridCut/bench-GridCut.cpp:76-100, built from the
+    reference sources under oracle/_ref), with every host thread, on the same
+    full workload as our arm: one step = graph init from the capacity arrays
+    + maxflow + labels into host memory.  Loads no part of the product."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent)"}))
         return
     cores = os.cpu_count() or 1
-    orc, shape, e, caps = reference_sample()
+    w, h = args.width, args.height
+    orc, shape, e, caps, sink = cpu_graph(w, h, replica_seed(0))
     n = e.size
+    labels = np.empty(n, np.uint8)
     for _ in range(args.warmup):
-        orc.gridcut_maxflow(shape, e, caps, cores)
-    times = []
+        orc.gridcut_maxflow(shape, e, caps, cores, labels)
+    times, parts, flows = [], np.zeros(3), set()
     for _ in range(args.steps):
-        f, t = orc.gridcut_maxflow(shape, e, caps, cores)
+        f, t = orc.gridcut_maxflow(shape, e, caps, cores, labels)
         times.append(sum(t))
+        parts += np.asarray(t)
+        flows.add(full_flow(e, f, sink))
     ms = 1000.0 * sum(times) / len(times)
     v = n / (ms / 1000.0) / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mnodes/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": "plain 2D 4-conn RGB ellipses, bounded CPU sample %dx%d" % (shape[1], shape[0]),
-                       "parallelism": "host threads"},
+            "config": {"workload": workload_name(w, h), "nodes": n, "global_batch": 1,
+                       "parallelism": "host threads x%d" % cores,
+                       "flow": flows.pop() if len(flows) == 1 else None,
+                       "ms_split_per_step": {k: 1000.0 * float(x) / args.steps
+                                             for k, x in zip(("init", "maxflow", "labels"), parts)}},
             "cpu_baseline": {"value": v, "unit": "Mnodes/s", "cores": cores, "kind": "reference",
-                             "sample": "GridCut 1.1 MT (reference benchmark/GridCut) on a %dx%d instance of the "
-                                       "workload, init+maxflow+labels per step" % (shape[1], shape[0])},
+                             "sample": "GridCut 1.1 MT (reference benchmark/GridCut) on the full %dx%d workload "
+                                       "graph, init + maxflow + labels per step" % (w, h)},
             "e2e": {"value": v, "unit": "Mnodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    print(json.dumps(line), flush=True)
 
 
-def cpu_baseline_bk():
-    """BK 3.03 (reference CPU path, 1 core) on a bounded sample, ~10-30 s."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+def cpu_baseline_bk(w, h, seed, flow_gpu):
+    """BK 3.03 (the reference's CPU path, benchmark/GridCut/bench-BK303.cpp,
+    1 core, int64 flow) on the full workload graph: one init + maxflow +
+    labels (~30 s and ~30 GB on the host)."""
     import oracle
     if not oracle.ref_available():
         return None
-    orc, shape, e, caps = reference_sample()
-    total, reps = 0.0, 0
-    while total < 10.0 and reps < 8:
-        f, _, t = orc.bk_maxflow(shape, e, caps, want_labels=True)
-        total += sum(t)
-        reps += 1
-    v = e.size * reps / total / 1e6
+    orc, shape, e, caps, sink = cpu_graph(w, h, seed)
+    f, lab, t = orc.bk_maxflow(shape, e, caps, want_labels=True)
+    v = e.size / sum(t) / 1e6
     return {"value": v, "unit": "Mnodes/s", "cores": 1, "kind": "reference",
-            "sample": "BK 3.03 (reference benchmark/GridCut/code/BK303, int64 flow) on a %dx%d instance of the "
-                      "workload x%d, init+maxflow+labels" % (shape[1], shape[0], reps)}
+            "sample": "BK 3.03 (reference benchmark/GridCut/code/BK303, int64 flow) on the full %dx%d workload "
+                      "graph, one init + maxflow + labels" % (w, h),
+            "s_split": {"init": t[0], "maxflow": t[1], "labels": t[2]},
+            "flow_equals_gpu": full_flow(e, f, sink) == flow_gpu}
 
 
 def max_over_ranks(x, dist=None, device="cuda"):
@@ -289,7 +311,7 @@ def bench_video(jfcut, torch, ctx, stream, steps=2, warmup=1, size=(2560, 1440, 
     and 49.  One step = capacity build from device-resident frames + solve +
     labels into a device buffer; flows must repeat exactly."""
     w, h, d = size
-    img, seeds = jfcut.synth_rgb_video(w, h, d, seed=SEED + 50)
+    img, seeds = synthetic.rgb_video(w, h, d, seed=SEED + 50)
     model = dict(MODEL, z_weight_pct=50)
     d_img = torch.from_numpy(img).cuda()
     d_seeds = torch.from_numpy(seeds).cuda()
@@ -365,13 +387,13 @@ def bench_serve(jfcut, torch, ctx, n_req=48, rate=200.0, budget_gb=96):
             pf = jfcut.PIX_RGB8
         else:
             w, h, d = (int(v) for v in rng.integers(128, 513, 3))
-            img, seeds = jfcut.synth_i16_phantom(w, h, d, seed=SEED + 9000 + i, noise_sigma=10)
+            img, seeds = synthetic.i16_phantom(w, h, d, seed=SEED + 9000 + i, noise_sigma=10)
             pf = jfcut.PIX_I16
         n = seeds.size
         edits = []
         for k in range(int(rng.integers(1, 6))):
             m = max(1, int(n * rng.uniform(0.001, 0.02)))
-            edits.append(jfcut.synth_stroke(seeds.shape, seed=SEED + 100 * i + k, n=m, label=1 + (k % 2)))
+            edits.append(synthetic.stroke(seeds.shape, seed=SEED + 100 * i + k, n=m, label=1 + (k % 2)))
         sess.append(dict(img=img, seeds=seeds, pf=pf, edits=edits, n=n, dims=seeds.ndim))
     srv = jfcut.Server(ctx, int(budget_gb * (1 << 30)), max_slots=64)
     records = []
@@ -442,7 +464,7 @@ def bench_edit4096(jfcut, torch, ctx, n_edits=100):
     edits = []
     for k in range(n_edits):
         m = max(1, int(w * h * rng.uniform(0.001, 0.02)))
-        edits.append(jfcut.synth_stroke(seeds.shape, seed=SEED + 7000 + k, n=m, label=1 + (k % 2)))
+        edits.append(synthetic.stroke(seeds.shape, seed=SEED + 7000 + k, n=m, label=1 + (k % 2)))
     srv = jfcut.Server(ctx, 0, max_slots=8)
     sid = srv.submit(img, seeds, jfcut.PIX_RGB8, MODEL)
     cold_first = srv.wait(sid).ms_total
@@ -594,8 +616,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "Mnodes/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": "plain: 2D 4-conn %dx%d RGB, 20 ellipses, N(0,15), 0.5%% strokes, 5-means "
-                                   "(build + solve + labels per step)" % (w, h),
+            "config": {"workload": workload_name(w, h),
                        "nodes": n, "global_batch": world, "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (state %.1f GB)" % (jfcut.lib().jfc_graph_bytes(2, w, h, 1) / 1e9),
                        "params": {"tile_rows": ctx.params().tile_rows, "local_iters": ctx.params().local_iters,
@@ -617,7 +638,7 @@ def main():
                                    % (bytes_per_visit, peak_kind)},
         }
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline_bk()
+            line["cpu_baseline"] = cpu_baseline_bk(w, h, replica_seed(rank), flow_ref)
         extras = [] if world > 1 or args.extras == "none" else args.extras.split(",")
         vsize = tuple(int(v) for v in args.video_size.split("x"))
         sections = {"video": lambda: bench_video(jfcut, torch, ctx, stream, size=vsize),

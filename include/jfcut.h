@@ -352,26 +352,6 @@ int jfc_load_mfi(const char* path, int32_t* excess, int32_t* const* ncap, int64_
 int jfc_save_mfi(const char* path, int dims, int w, int h, int d, const int32_t* excess, const int32_t* const* ncap,
                  int64_t maxflow, const uint8_t* mask);
 
-/* ---- synthetic inputs (seeded, deterministic, integer arithmetic) used by the
- * tests and the benchmark in place of the reference's image files ---- */
-/* 2D gray: blurred ellipse (fg 170 / bg 80) + N(0,sigma) noise, 1-px strokes. */
-int jfc_synth_gray_ellipse(int w, int h, uint64_t seed, int noise_sigma,
-                           uint8_t* img, uint8_t* seeds);
-/* 2D RGB: n_ellipses random overlapping ellipses, region means U(0,255)^3,
- * N(0,noise_sigma) noise, random strokes covering stroke_permille/1000 of pixels. */
-int jfc_synth_rgb_ellipses(int w, int h, uint64_t seed, int n_ellipses, int noise_sigma,
-                           int stroke_permille_x10, uint8_t* img, uint8_t* seeds);
-/* 3D RGB video: ellipse moving 4 px/frame over value-noise texture; strokes on
- * the first and last frame. */
-int jfc_synth_rgb_video(int w, int h, int frames, uint64_t seed, uint8_t* img, uint8_t* seeds);
-/* 3D int16 volume: sphere-and-tube phantom + N(0,noise_sigma) noise; seed blobs. */
-int jfc_synth_i16_phantom(int w, int h, int d, uint64_t seed, int noise_sigma,
-                          int16_t* img, uint8_t* seeds);
-/* Random brush stroke: a seeded walk over up to n distinct nodes, all given
- * seed value `label`; *n_out receives the number of nodes written. */
-int jfc_synth_stroke(int dims, int w, int h, int d, uint64_t seed, size_t n, uint8_t label,
-                     uint32_t* idx, uint8_t* new_seed, size_t* n_out);
-
 #ifdef __cplusplus
 }
 #endif

@@ -177,15 +177,6 @@ def _lib():
         L.jfc_read_mfi_info.argtypes = [CP, ctypes.POINTER(MfiInfo)]
         L.jfc_load_mfi.argtypes = [CP, I32P, ctypes.POINTER(I32P), ctypes.POINTER(ctypes.c_int64), U8P]
         L.jfc_save_mfi.argtypes = [CP] + [ctypes.c_int] * 4 + [I32P, ctypes.POINTER(I32P), ctypes.c_int64, U8P]
-        L.jfc_synth_gray_ellipse.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int, U8P, U8P]
-        L.jfc_synth_rgb_ellipses.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
-                                             ctypes.c_int, ctypes.c_int, U8P, U8P]
-        L.jfc_synth_rgb_video.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64, U8P, U8P]
-        L.jfc_synth_i16_phantom.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
-                                            ctypes.c_int, ctypes.POINTER(ctypes.c_int16), U8P]
-        L.jfc_synth_stroke.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
-                                       ctypes.c_size_t, ctypes.c_uint8, U32P, U8P,
-                                       ctypes.POINTER(ctypes.c_size_t)]
         _LIB = L
     return _LIB
 
@@ -240,6 +231,11 @@ class Context:
         p = self.params()
         for k, v in params.items():
             setattr(p, k, int(v))
+        _check(_lib().jfc_set_params(self.handle, ctypes.byref(p)), "jfc_set_params")
+
+    def reset_params(self):
+        """Back to the library's default schedule (jfc_default_params)."""
+        p = default_params()
         _check(_lib().jfc_set_params(self.handle, ctypes.byref(p)), "jfc_set_params")
 
     def set_stream(self, stream_ptr):
@@ -636,48 +632,3 @@ def graph_bytes(shape):
     if len(shape) == 2:
         return int(_lib().jfc_graph_bytes(2, int(shape[1]), int(shape[0]), 1))
     return int(_lib().jfc_graph_bytes(3, int(shape[2]), int(shape[1]), int(shape[0])))
-
-
-# ---------------------------------------------------------------- synthetic inputs
-def synth_gray_ellipse(w, h, seed=0, noise_sigma=20):
-    img = np.empty((h, w), np.uint8)
-    seeds = np.empty((h, w), np.uint8)
-    _check(_lib().jfc_synth_gray_ellipse(w, h, seed, noise_sigma, _p(img, U8P), _p(seeds, U8P)),
-           "jfc_synth_gray_ellipse")
-    return img, seeds
-
-
-def synth_rgb_ellipses(w, h, seed=0, n_ellipses=20, noise_sigma=15, stroke_permille_x10=50):
-    img = np.empty((h, w, 3), np.uint8)
-    seeds = np.empty((h, w), np.uint8)
-    _check(_lib().jfc_synth_rgb_ellipses(w, h, seed, n_ellipses, noise_sigma, stroke_permille_x10,
-                                         _p(img, U8P), _p(seeds, U8P)), "jfc_synth_rgb_ellipses")
-    return img, seeds
-
-
-def synth_rgb_video(w, h, frames, seed=0):
-    img = np.empty((frames, h, w, 3), np.uint8)
-    seeds = np.empty((frames, h, w), np.uint8)
-    _check(_lib().jfc_synth_rgb_video(w, h, frames, seed, _p(img, U8P), _p(seeds, U8P)), "jfc_synth_rgb_video")
-    return img, seeds
-
-
-def synth_i16_phantom(w, h, d, seed=0, noise_sigma=10):
-    img = np.empty((d, h, w), np.int16)
-    seeds = np.empty((d, h, w), np.uint8)
-    _check(_lib().jfc_synth_i16_phantom(w, h, d, seed, noise_sigma, img.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)),
-                                        _p(seeds, U8P)), "jfc_synth_i16_phantom")
-    return img, seeds
-
-
-def synth_stroke(shape, seed, n, label):
-    if len(shape) == 2:
-        dims, (h, w), d = 2, shape, 1
-    else:
-        dims, (d, h, w) = 3, shape
-    idx = np.empty(n, np.uint32)
-    ns = np.empty(n, np.uint8)
-    k = ctypes.c_size_t(0)
-    _check(_lib().jfc_synth_stroke(dims, w, h, d, seed, n, label, _p(idx, U32P), _p(ns, U8P), ctypes.byref(k)),
-           "jfc_synth_stroke")
-    return idx[:k.value].copy(), ns[:k.value].copy()

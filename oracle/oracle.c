@@ -110,6 +110,7 @@ void orc_contrast_sum(int dims, int w, int h, int d, int pixfmt, const void* img
   grid_t g; grid_init(&g, dims, w, h, d);
   uint64_t s = 0, c = 0;
   int npos = g.conn / 2;   /* +x, +y (, +z) */
+#pragma omp parallel for schedule(static) reduction(+ : s, c)
   for (int64_t i = 0; i < g.n; ++i)
     for (int k = 0; k < npos; ++k) {
       if (!arc_ok(&g, i, k)) continue;
@@ -143,12 +144,21 @@ static void kmeans_class(int pixfmt, const void* img, const uint8_t* seeds, int6
   int C = pix_channels(pixfmt);
   int mn[3] = {1 << 30, 1 << 30, 1 << 30}, mx[3] = {-1, -1, -1};
   int f[3];
+  /* the class's seed features, gathered once (node order) */
+  int64_t m = 0;
+  for (int64_t i = 0; i < n; ++i) m += seeds[i] == cls;
+  int* feats = (int*)malloc(sizeof(int) * 3 * (size_t)(m ? m : 1));
+  m = 0;
   for (int64_t i = 0; i < n; ++i) {
     if (seeds[i] != cls) continue;
-    pix_feat(pixfmt, img, i, f);
+    pix_feat(pixfmt, img, i, feats + 3 * m);
+    ++m;
+  }
+  for (int64_t j = 0; j < m; ++j) {
+    const int* fj = feats + 3 * j;
     for (int c = 0; c < C; ++c) {
-      if (f[c] < mn[c]) mn[c] = f[c];
-      if (f[c] > mx[c]) mx[c] = f[c];
+      if (fj[c] < mn[c]) mn[c] = fj[c];
+      if (fj[c] > mx[c]) mx[c] = fj[c];
     }
   }
   for (int j = 0; j < k; ++j)
@@ -159,9 +169,8 @@ static void kmeans_class(int pixfmt, const void* img, const uint8_t* seeds, int6
   int64_t* sums = (int64_t*)calloc((size_t)k * 4, sizeof(int64_t));
   for (int it = 0; it < iters; ++it) {
     memset(sums, 0, (size_t)k * 4 * sizeof(int64_t));
-    for (int64_t i = 0; i < n; ++i) {
-      if (seeds[i] != cls) continue;
-      pix_feat(pixfmt, img, i, f);
+    for (int64_t j = 0; j < m; ++j) {
+      for (int c = 0; c < 3; ++c) f[c] = feats[3 * j + c];
       int best = 0;
       int64_t bd = feat_dist(f, mu, C);
       for (int j = 1; j < k; ++j) {
@@ -183,6 +192,7 @@ static void kmeans_class(int pixfmt, const void* img, const uint8_t* seeds, int6
     if (!moved) break;
   }
   free(sums);
+  free(feats);
 }
 
 static int64_t min_dist(const int* f, const int32_t* mu, int k, int C) {
@@ -194,9 +204,14 @@ static int64_t min_dist(const int* f, const int32_t* mu, int k, int C) {
   return bd;
 }
 
-int orc_build_graph(int dims, int w, int h, int d, int pixfmt, const void* img,
-                    const uint8_t* seeds, const orc_model* m, int32_t* e,
-                    int32_t* const* caps, int64_t* sink_total, int32_t* centroids_out) {
+/* Capacity build with the colour models fit on seeds_model and the t-links
+ * set from seeds_tl.  With seeds_tl == seeds_model this is the plain build;
+ * with the seeds of a session after stroke edits it is the graph the warm
+ * edit path holds (an edit recomputes the edited nodes' t-links with the
+ * session's colour model, which stays the one of the original strokes). */
+int orc_build_graph_ex(int dims, int w, int h, int d, int pixfmt, const void* img,
+                       const uint8_t* seeds, const uint8_t* seeds_tl, const orc_model* m, int32_t* e,
+                       int32_t* const* caps, int64_t* sink_total, int32_t* centroids_out) {
   grid_t g; grid_init(&g, dims, w, h, d);
   int C = pix_channels(pixfmt);
   int64_t nfg = 0, nbg = 0;
@@ -212,14 +227,27 @@ int orc_build_graph(int dims, int w, int h, int d, int pixfmt, const void* img,
   double sigma2 = scnt ? (double)ssum / (double)scnt : 0.0;
   double scale_xy = (double)m->lambda_n;
   double scale_z = (double)m->lambda_n * (double)m->z_weight_pct / 100.0;
+  /* 8-bit images: D < 3 * 256^2, so the weights are tabulated once (the same
+   * values nlink_weight gives); int16 volumes evaluate it per arc */
+  const int64_t dmax = pixfmt == 2 ? 0 : 3 * 256 * 256;
+  int32_t* wt_xy = dmax ? (int32_t*)malloc(sizeof(int32_t) * (size_t)dmax) : NULL;
+  int32_t* wt_z = dmax ? (int32_t*)malloc(sizeof(int32_t) * (size_t)dmax) : NULL;
+  for (int64_t v = 0; v < dmax; ++v) {
+    wt_xy[v] = nlink_weight(scale_xy, sigma2, (uint64_t)v);
+    wt_z[v] = nlink_weight(scale_z, sigma2, (uint64_t)v);
+  }
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < g.n; ++i)
     for (int k = 0; k < g.conn; ++k) {
       if (!arc_ok(&g, i, k)) { caps[k][i] = 0; continue; }
       int64_t idx; uint64_t dsq;
       pair_contrast(pixfmt, img, i, i + g.off[k], &idx, &dsq);
       int zdir = (g.dims == 3) && (k == 2 || k == 3);
-      caps[k][i] = nlink_weight(zdir ? scale_z : scale_xy, sigma2, dsq);
+      caps[k][i] = (int64_t)dsq < dmax ? (zdir ? wt_z : wt_xy)[dsq]
+                                       : nlink_weight(zdir ? scale_z : scale_xy, sigma2, dsq);
     }
+  free(wt_xy);
+  free(wt_z);
 
   /* colour models (fg / bg) */
   int kf = m->k_fg < 1 ? 1 : m->k_fg, kb = m->k_bg < 1 ? 1 : m->k_bg;
@@ -245,11 +273,12 @@ int orc_build_graph(int dims, int w, int h, int d, int pixfmt, const void* img,
     lut_t[q] = (int32_t)floor((double)m->lambda_t * -log(pf) + 0.5);
   }
   int64_t st = 0;
-  int f[3];
+#pragma omp parallel for schedule(static) reduction(+ : st)
   for (int64_t i = 0; i < g.n; ++i) {
+    int f[3];
     int32_t cs, ct;
-    if (seeds[i] == 1) { cs = m->seed_cap; ct = 0; }
-    else if (seeds[i] == 2) { cs = 0; ct = m->seed_cap; }
+    if (seeds_tl[i] == 1) { cs = m->seed_cap; ct = 0; }
+    else if (seeds_tl[i] == 2) { cs = 0; ct = m->seed_cap; }
     else {
       pix_feat(pixfmt, img, i, f);
       uint64_t dF = (uint64_t)min_dist(f, muF, kf, C);
@@ -263,6 +292,12 @@ int orc_build_graph(int dims, int w, int h, int d, int pixfmt, const void* img,
   free(lut_s); free(lut_t);
   *sink_total = st;
   return 0;
+}
+
+int orc_build_graph(int dims, int w, int h, int d, int pixfmt, const void* img,
+                    const uint8_t* seeds, const orc_model* m, int32_t* e,
+                    int32_t* const* caps, int64_t* sink_total, int32_t* centroids_out) {
+  return orc_build_graph_ex(dims, w, h, d, pixfmt, img, seeds, seeds, m, e, caps, sink_total, centroids_out);
 }
 
 /* ------------------------------------------------------------- max-flow */

@@ -32,6 +32,12 @@ int orc_build_graph(int dims, int w, int h, int d, int pixfmt, const void* img,
                     const uint8_t* seeds, const orc_model* m, int32_t* e,
                     int32_t* const* caps, int64_t* sink_total, int32_t* centroids_out);
 
+/* The same build with the colour models fit on `seeds` and the t-links set
+ * from `seeds_tl` (the graph a session holds after warm stroke edits). */
+int orc_build_graph_ex(int dims, int w, int h, int d, int pixfmt, const void* img,
+                       const uint8_t* seeds, const uint8_t* seeds_tl, const orc_model* m, int32_t* e,
+                       int32_t* const* caps, int64_t* sink_total, int32_t* centroids_out);
+
 /* Sum of squared neighbour differences and pair count (sigma^2 = sum/count). */
 void orc_contrast_sum(int dims, int w, int h, int d, int pixfmt, const void* img,
                       uint64_t* sum, uint64_t* count);

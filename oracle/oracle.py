@@ -37,6 +37,7 @@ def lib():
             build()
         L = ctypes.CDLL(path)
         L.orc_build_graph.restype = ctypes.c_int
+        L.orc_build_graph_ex.restype = ctypes.c_int
         L.orc_maxflow.restype = ctypes.c_int64
         L.orc_cut_from_residual.restype = ctypes.c_int64
         L.orc_cut_energy.restype = ctypes.c_int64
@@ -73,9 +74,12 @@ def _shape(shape):
     return 3, w, h, d
 
 
-def build_graph(img, seeds, pixfmt, model):
+def build_graph(img, seeds, pixfmt, model, seeds_tl=None):
     """Capacity build.  img: (H,W)/(H,W,3)/(D,H,W) array; seeds same grid.
-    Returns (e, caps[conn], sink_total) or raises on missing seeds."""
+    Returns (e, caps[conn], sink_total) or raises on missing seeds.
+    seeds_tl: the seeds after stroke edits — the colour models are fit on
+    `seeds`, the t-links follow `seeds_tl` (the graph a warm-edited session
+    holds)."""
     shape = seeds.shape
     dims, w, h, d = _shape(shape)
     conn = 4 if dims == 2 else 6
@@ -88,9 +92,10 @@ def build_graph(img, seeds, pixfmt, model):
                                             "seed_cap", "kmeans_iters")])
     img = np.ascontiguousarray(img)
     seeds = np.ascontiguousarray(seeds, dtype=np.uint8)
-    rc = lib().orc_build_graph(dims, w, h, d, pixfmt, img.ctypes.data_as(ctypes.c_void_p),
-                               seeds.ctypes.data_as(U8P), ctypes.byref(m),
-                               e.ctypes.data_as(I32P), P, ctypes.byref(st), None)
+    tl = seeds if seeds_tl is None else np.ascontiguousarray(seeds_tl, dtype=np.uint8).reshape(seeds.shape)
+    rc = lib().orc_build_graph_ex(dims, w, h, d, pixfmt, img.ctypes.data_as(ctypes.c_void_p),
+                                  seeds.ctypes.data_as(U8P), tl.ctypes.data_as(U8P), ctypes.byref(m),
+                                  e.ctypes.data_as(I32P), P, ctypes.byref(st), None)
     if rc != 0:
         raise ValueError("oracle build failed: %d" % rc)
     return e, caps, st.value
@@ -160,10 +165,14 @@ def bk_maxflow(shape, e, caps, want_labels=True):
     return int(f), lab, tuple(times)
 
 
-def gridcut_maxflow(shape, e, caps, threads):
+def gridcut_maxflow(shape, e, caps, threads, labels=None):
+    """Reference GridCut 1.1 multi-threaded.  Returns (folded flow,
+    (t_init, t_maxflow, t_output)); `labels` (uint8 array of the grid's size,
+    optional) receives the source side GridCut reports."""
     dims, w, h, d = _shape(shape)
     e = np.ascontiguousarray(e, dtype=np.int32)
     keep, P = _ptrs(caps)
     times = (ctypes.c_double * 3)()
-    f = ref().ref_gridcut_maxflow(dims, w, h, d, e.ctypes.data_as(I32P), P, int(threads), times)
+    lp = labels.ctypes.data_as(U8P) if labels is not None else None
+    f = ref().ref_gridcut_maxflow(dims, w, h, d, e.ctypes.data_as(I32P), P, int(threads), lp, times)
     return int(f), tuple(times)

@@ -68,8 +68,10 @@ long long ref_bk_maxflow(int dims, int w, int h, int d, const int32_t* e,
 
 // GridCut 1.1 multi-threaded (the reference harness's MT path,
 // bench-GridCut.cpp:76-216, block_size rule from :92/:192).  Folded flow.
+// labels (may be NULL): 1 where get_segment reports the source side
+// (GridGraph_2D_4C_MT.h:1152-1157); times[2] covers that read-back.
 long long ref_gridcut_maxflow(int dims, int w, int h, int d, const int32_t* e,
-                              const int32_t* const* caps, int threads, double* times) {
+                              const int32_t* const* caps, int threads, uint8_t* labels, double* times) {
   if (dims == 2) d = 1;
   const long long n = (long long)w * h * d;
   if (threads < 1) threads = 1;
@@ -91,6 +93,9 @@ long long ref_gridcut_maxflow(int dims, int w, int h, int d, const int32_t* e,
     g->compute_maxflow();
     t2 = now_s();
     flow = g->get_flow();
+    if (labels)
+      for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) labels[(long long)y * w + x] = g->get_segment(g->node_id(x, y)) == 0;
     delete g;
   } else {
     typedef GridGraph_3D_6C_MT<int, int, long long> G;
@@ -102,6 +107,11 @@ long long ref_gridcut_maxflow(int dims, int w, int h, int d, const int32_t* e,
     g->compute_maxflow();
     t2 = now_s();
     flow = g->get_flow();
+    if (labels)
+      for (int z = 0; z < d; ++z)
+        for (int y = 0; y < h; ++y)
+          for (int x = 0; x < w; ++x)
+            labels[(long long)w * h * z + (long long)y * w + x] = g->get_segment(g->node_id(x, y, z)) == 0;
     delete g;
   }
   double t3 = now_s();

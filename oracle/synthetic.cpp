@@ -1,4 +1,11 @@
-// synth.cpp — seeded synthetic inputs for the tests and the benchmark.
+// synthetic.cpp — seeded synthetic inputs for the tests and both bench arms.
+//
+// INPUT GENERATION ONLY: the tests, __graft_entry__.smoke() and bench.py call
+// these before any timed region to make the images, videos, volumes and
+// strokes the workloads name; nothing on the solve path (libjfcut.so,
+// jfcut.py) links or calls them.  They live beside the CPU checker so that
+// bench.py's reference arm can build the same graph from the same bytes
+// without loading the product library.
 //
 // The reference reads image / volume files and user brush strokes
 // (QGCWidget.cpp:296-683, 2243-2287); the benchmark configurations here are
@@ -13,9 +20,11 @@
 #include <unordered_set>
 #include <vector>
 
-#include "../../include/jfcut.h"
 
 namespace {
+
+constexpr int SYN_OK = 0, SYN_ERR_INVALID_ARG = 1;   // status codes
+constexpr uint8_t SEED_FG = 1, SEED_BG = 2;           // seed bytes (0: none)
 
 inline uint64_t mix64(uint64_t z) {
   z += 0x9e3779b97f4a7c15ull;
@@ -69,8 +78,8 @@ struct Ellipse {
 
 extern "C" {
 
-int jfc_synth_gray_ellipse(int w, int h, uint64_t seed, int noise_sigma, uint8_t* img, uint8_t* seeds) {
-  if (w < 8 || h < 8 || !img || !seeds) return JFC_ERR_INVALID_ARG;
+int syn_gray_ellipse(int w, int h, uint64_t seed, int noise_sigma, uint8_t* img, uint8_t* seeds) {
+  if (w < 8 || h < 8 || !img || !seeds) return SYN_ERR_INVALID_ARG;
   const long long cx = w / 2, cy = h / 2, a = w / 4, b = h / 5;
   const size_t n = (size_t)w * h;
   std::vector<int> mask(n), tmp(n);
@@ -97,15 +106,15 @@ int jfc_synth_gray_ellipse(int w, int h, uint64_t seed, int noise_sigma, uint8_t
       img[(size_t)y * w + x] = (uint8_t)clip255(v);
     }
   std::memset(seeds, 0, n);
-  for (long long x = cx - a / 2; x <= cx + a / 2; ++x) seeds[(size_t)cy * w + x] = JFC_SEED_FG;
+  for (long long x = cx - a / 2; x <= cx + a / 2; ++x) seeds[(size_t)cy * w + x] = SEED_FG;
   const int yb = h / 10;
-  for (int x = w / 4; x < 3 * w / 4; ++x) seeds[(size_t)yb * w + x] = JFC_SEED_BG;
-  return JFC_OK;
+  for (int x = w / 4; x < 3 * w / 4; ++x) seeds[(size_t)yb * w + x] = SEED_BG;
+  return SYN_OK;
 }
 
-int jfc_synth_rgb_ellipses(int w, int h, uint64_t seed, int n_ellipses, int noise_sigma, int stroke_permille_x10,
+int syn_rgb_ellipses(int w, int h, uint64_t seed, int n_ellipses, int noise_sigma, int stroke_permille_x10,
                            uint8_t* img, uint8_t* seeds) {
-  if (w < 8 || h < 8 || !img || !seeds || n_ellipses < 1 || n_ellipses > 256) return JFC_ERR_INVALID_ARG;
+  if (w < 8 || h < 8 || !img || !seeds || n_ellipses < 1 || n_ellipses > 256) return SYN_ERR_INVALID_ARG;
   Rng rng(seed);
   const int mside = std::min(w, h);
   int bgcol[3];
@@ -150,7 +159,7 @@ int jfc_synth_rgb_ellipses(int w, int h, uint64_t seed, int n_ellipses, int nois
     const bool fg = rg >= 0 && el[rg].fg;
     if (have[0] && have[1] && marked >= target) break;
     if (marked >= target && have[fg ? 0 : 1]) continue;
-    const int lab = fg ? JFC_SEED_FG : JFC_SEED_BG;
+    const int lab = fg ? SEED_FG : SEED_BG;
     const int* d = dirs[rng.uni(0, 7)];
     const int len = rng.uni(16, 128);
     for (int s = 0; s < len; ++s) {
@@ -162,11 +171,11 @@ int jfc_synth_rgb_ellipses(int w, int h, uint64_t seed, int n_ellipses, int nois
       x += d[0]; y += d[1];
     }
   }
-  return JFC_OK;
+  return SYN_OK;
 }
 
-int jfc_synth_rgb_video(int w, int h, int frames, uint64_t seed, uint8_t* img, uint8_t* seeds) {
-  if (w < 32 || h < 32 || frames < 2 || !img || !seeds) return JFC_ERR_INVALID_ARG;
+int syn_rgb_video(int w, int h, int frames, uint64_t seed, uint8_t* img, uint8_t* seeds) {
+  if (w < 32 || h < 32 || frames < 2 || !img || !seeds) return SYN_ERR_INVALID_ARG;
   Rng rng(seed);
   const int cell = 32;
   const int gw = w / cell + 2, gh = h / cell + 2;
@@ -207,17 +216,17 @@ int jfc_synth_rgb_video(int w, int h, int frames, uint64_t seed, uint8_t* img, u
   for (int z : {0, frames - 1}) {
     const long long cx = cx0 + 4ll * z;
     for (long long x = cx - a / 2; x <= cx + a / 2; ++x)
-      if (x >= 0 && x < w) seeds[(size_t)z * wh + (size_t)cy * w + x] = JFC_SEED_FG;
+      if (x >= 0 && x < w) seeds[(size_t)z * wh + (size_t)cy * w + x] = SEED_FG;
     for (int x = w / 8; x < 7 * w / 8; ++x) {
-      seeds[(size_t)z * wh + (size_t)(h / 12) * w + x] = JFC_SEED_BG;
-      seeds[(size_t)z * wh + (size_t)(h - 1 - h / 12) * w + x] = JFC_SEED_BG;
+      seeds[(size_t)z * wh + (size_t)(h / 12) * w + x] = SEED_BG;
+      seeds[(size_t)z * wh + (size_t)(h - 1 - h / 12) * w + x] = SEED_BG;
     }
   }
-  return JFC_OK;
+  return SYN_OK;
 }
 
-int jfc_synth_i16_phantom(int w, int h, int d, uint64_t seed, int noise_sigma, int16_t* img, uint8_t* seeds) {
-  if (w < 8 || h < 8 || d < 8 || !img || !seeds) return JFC_ERR_INVALID_ARG;
+int syn_i16_phantom(int w, int h, int d, uint64_t seed, int noise_sigma, int16_t* img, uint8_t* seeds) {
+  if (w < 8 || h < 8 || d < 8 || !img || !seeds) return SYN_ERR_INVALID_ARG;
   const long long cx = w / 2, cy = h / 2, cz = d / 2;
   const long long R = std::min(std::min(w, h), d) / 4;
   const long long tr = std::max<long long>(2, R / 3);
@@ -239,16 +248,16 @@ int jfc_synth_i16_phantom(int w, int h, int d, uint64_t seed, int noise_sigma, i
   const long long s = std::max<long long>(1, R / 4);
   for (long long z = cz - s; z <= cz + s; ++z)
     for (long long y = cy - s; y <= cy + s; ++y)
-      for (long long x = cx - s; x <= cx + s; ++x) seeds[(size_t)z * wh + (size_t)y * w + x] = JFC_SEED_FG;
+      for (long long x = cx - s; x <= cx + s; ++x) seeds[(size_t)z * wh + (size_t)y * w + x] = SEED_FG;
   for (long long z = 1; z <= 1 + s; ++z)
     for (long long y = 1; y <= 1 + s; ++y)
-      for (long long x = 1; x <= 1 + s; ++x) seeds[(size_t)z * wh + (size_t)y * w + x] = JFC_SEED_BG;
-  return JFC_OK;
+      for (long long x = 1; x <= 1 + s; ++x) seeds[(size_t)z * wh + (size_t)y * w + x] = SEED_BG;
+  return SYN_OK;
 }
 
-int jfc_synth_stroke(int dims, int w, int h, int d, uint64_t seed, size_t n, uint8_t label, uint32_t* idx,
+int syn_stroke(int dims, int w, int h, int d, uint64_t seed, size_t n, uint8_t label, uint32_t* idx,
                      uint8_t* new_seed, size_t* n_out) {
-  if (!idx || !new_seed || !n_out || w < 1 || h < 1) return JFC_ERR_INVALID_ARG;
+  if (!idx || !new_seed || !n_out || w < 1 || h < 1) return SYN_ERR_INVALID_ARG;
   if (dims == 2) d = 1;
   Rng rng(seed);
   std::unordered_set<uint64_t> seen;
@@ -269,7 +278,7 @@ int jfc_synth_stroke(int dims, int w, int h, int d, uint64_t seed, size_t n, uin
     x = nx; y = ny; z = nz;
   }
   *n_out = k;
-  return JFC_OK;
+  return SYN_OK;
 }
 
 }  // extern "C"

@@ -26,7 +26,7 @@ def pytest_configure(config):
 def _ensure_built():
     if not os.path.exists(os.path.join(PKG, "libjfcut.so")):
         subprocess.run(["make", "-s", "-j8", "-C", PKG], check=True)
-    if not os.path.exists(os.path.join(ORACLE, "liboracle.so")):
+    if not all(os.path.exists(os.path.join(ORACLE, f)) for f in ("liboracle.so", "libsynthetic.so")):
         subprocess.run(["make", "-s", "-f", os.path.join(ORACLE, "Makefile")], check=True, cwd=ORACLE)
 
 
@@ -86,3 +86,34 @@ def ctx():
     c = jfcut.Context(0)
     yield c
     c.close()
+
+
+@pytest.fixture(autouse=True)
+def _default_schedule(request):
+    """Every test that uses the shared context starts, and leaves it, on the
+    library's default schedule (the one bench.py times): a test that changes
+    the schedule cannot leak it into the tests after it."""
+    if "ctx" not in request.fixturenames:
+        yield
+        return
+    c = request.getfixturevalue("ctx")
+    c.reset_params()
+    yield
+    c.reset_params()
+
+
+# Schedules the parity tests run under: the default (32 x 8 tiles, 12 rounds
+# per visit, automatic relabel interval), 32 x 16 relabel tiles with
+# push-relabel on their 32 x 8 halves, and whole 32 x 16 push-relabel tiles.
+SCHEDULES = {"default": {}, "rows16": dict(tile_rows=16), "whole16": dict(tile_rows=16, pr_mode=2)}
+
+
+def use_schedule(ctx, name):
+    """Switch the shared context to a named schedule; for "default" also check
+    that the context really is on the library defaults."""
+    import jfcut
+    if name == "default":
+        p, d = ctx.params(), jfcut.default_params()
+        assert all(getattr(p, f) == getattr(d, f) for f, _ in p._fields_), "context is not on the defaults"
+    else:
+        ctx.set_params(**SCHEDULES[name])

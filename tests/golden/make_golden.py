@@ -8,7 +8,7 @@ compressed together with the published max-flow values
 (cl_cut.object, non-zero only in flower's file).
 
 Run in a container that has the reference tree:
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>     (or JFC_REFERENCE=<checkout>)
 """
 import os
 import sys
@@ -53,4 +53,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("JFC_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py <reference checkout>   (or set JFC_REFERENCE)")
+    main(root)

@@ -11,8 +11,9 @@ import jfcut
 import oracle
 from conftest import FIXTURES, load_fixture, random_grid
 
-REF_DATA = "/root/reference/src/QVisualizer/data"
-have_ref = os.path.isdir(REF_DATA)
+# the reference checkout, when JFC_REFERENCE names it: its data files are read directly
+REF_DATA = os.path.join(os.environ.get("JFC_REFERENCE", ""), "src", "QVisualizer", "data")
+have_ref = bool(os.environ.get("JFC_REFERENCE")) and os.path.isdir(REF_DATA)
 
 
 def test_graph_files_round_trip(tmp_path):

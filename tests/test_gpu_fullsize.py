@@ -13,6 +13,7 @@ import pytest
 
 import jfcut
 import oracle
+import synthetic
 
 pytestmark = [pytest.mark.gpu, pytest.mark.slow]
 
@@ -21,10 +22,10 @@ MODEL5 = dict(lambda_n=100, z_weight_pct=100, lambda_t=10, k_fg=5, k_bg=5, seed_
 
 def _workload(kind):
     if kind == "plain":
-        img, seeds = jfcut.synth_rgb_ellipses(15000, 10000, seed=20240601, n_ellipses=20, noise_sigma=15,
+        img, seeds = synthetic.rgb_ellipses(15000, 10000, seed=20240601, n_ellipses=20, noise_sigma=15,
                                               stroke_permille_x10=50)
         return img, seeds, MODEL5
-    img, seeds = jfcut.synth_rgb_video(2560, 1440, 50, seed=20240601 + 50)
+    img, seeds = synthetic.rgb_video(2560, 1440, 50, seed=20240601 + 50)
     return img, seeds, dict(MODEL5, z_weight_pct=50)
 
 

@@ -1,7 +1,8 @@
 """GPU: the serving loop (continuous batching, HBM-budget admission, warm
-stroke edits).  Every result must be bit-identical to the plain solver's on
-the same graph, whether the request ran alone or shared its launches with
-others."""
+stroke edits).  Every result, cold or warm-edited, 2D or 3D, must be
+bit-identical to the CPU oracle's max-flow and canonical cut of the same graph
+(and so to the plain solver's), whether the request ran alone or shared its
+launches with others."""
 import threading
 import time
 
@@ -9,6 +10,8 @@ import numpy as np
 import pytest
 
 import jfcut
+import oracle
+import synthetic
 
 pytestmark = pytest.mark.gpu
 
@@ -22,14 +25,14 @@ def make_requests(seed, n2d, n3d, lo=24, hi=400):
     for i in range(n2d):
         w, h = (int(v) for v in rng.integers(lo, hi, 2))
         if i % 2 == 0:
-            img, seeds = jfcut.synth_rgb_ellipses(w, h, seed=seed * 1000 + i)
+            img, seeds = synthetic.rgb_ellipses(w, h, seed=seed * 1000 + i)
             reqs.append((img, seeds, jfcut.PIX_RGB8, MODEL5))
         else:
-            img, seeds = jfcut.synth_gray_ellipse(w, h, seed=seed * 1000 + i)
+            img, seeds = synthetic.gray_ellipse(w, h, seed=seed * 1000 + i)
             reqs.append((img, seeds, jfcut.PIX_GRAY8, MODEL2))
     for j in range(n3d):
         w, h, d = (int(v) for v in rng.integers(16, 48, 3))
-        img, seeds = jfcut.synth_i16_phantom(w, h, d, seed=seed * 1000 + 500 + j)
+        img, seeds = synthetic.i16_phantom(w, h, d, seed=seed * 1000 + 500 + j)
         reqs.append((img, seeds, jfcut.PIX_I16, MODEL2))
     return reqs
 
@@ -40,13 +43,26 @@ def strokes(shape, seed, count):
     out = []
     for k in range(count):
         m = max(1, int(n * rng.uniform(0.001, 0.02)))
-        out.append(jfcut.synth_stroke(shape, seed=seed * 10 + k, n=m, label=1 + (k % 2)))
+        out.append(synthetic.stroke(shape, seed=seed * 10 + k, n=m, label=1 + (k % 2)))
     return out
+
+
+def cpu_oracle(img, seeds, pf, model, edits=()):
+    """The CPU oracle on the graph a session holds after `edits`: colour
+    models fit on the original seeds, t-links from the edited seeds; returns
+    the full int64 max-flow and the canonical source side."""
+    cur = seeds.ravel().copy()
+    for idx, ns in edits:
+        cur[idx] = ns
+    e, caps, sink = oracle.build_graph(img, seeds, pf, model, seeds_tl=cur)
+    _, ef, _, lab = oracle.maxflow(seeds.shape, e, caps)
+    return sink + int(np.minimum(ef.astype(np.int64), 0).sum()), lab.reshape(seeds.shape)
 
 
 def plain(ctx, img, seeds, pf, model, edits=()):
     """Cold reference: build, apply every edit so far (the colour model stays
-    the one of the original seeds, as on the warm path), solve from scratch."""
+    the one of the original seeds, as on the warm path), solve from scratch
+    with the plain solver; both it and the server are held to the CPU oracle."""
     g = jfcut.Graph(ctx, seeds.shape)
     g.build_from_image(img, seeds, pf, model)
     for idx, ns in edits:
@@ -54,7 +70,10 @@ def plain(ctx, img, seeds, pf, model, edits=()):
     g.solve()
     out = g.flow(), g.labels().copy()
     g.close()
-    return out
+    want = cpu_oracle(img, seeds, pf, model, edits)
+    assert out[0] == want[0]
+    assert np.array_equal(out[1], want[1])
+    return want
 
 
 def test_mix_equals_alone_with_warm_edits(ctx):
@@ -97,6 +116,8 @@ def test_alone_in_server_equals_mix(ctx):
         info = srv.wait(sid)
         alone.append((info.flow, srv.labels(sid, seeds.shape)))
         srv.close()
+        flow, lab = cpu_oracle(img, seeds, pf, model)
+        assert alone[-1][0] == flow and np.array_equal(alone[-1][1], lab)
     srv = jfcut.Server(ctx, 0, max_slots=64)
     try:
         sids = [srv.submit(*r) for r in reqs]
@@ -115,7 +136,7 @@ def test_budget_admission(ctx):
     srv = jfcut.Server(ctx, budget, max_slots=64)
     try:
         # a session that can never fit is refused up front
-        img, seeds = jfcut.synth_rgb_ellipses(2000, 2000, seed=1)
+        img, seeds = synthetic.rgb_ellipses(2000, 2000, seed=1)
         with pytest.raises(jfcut.JfcError) as ex:
             srv.submit(img, seeds, jfcut.PIX_RGB8, MODEL5)
         assert ex.value.code == jfcut.ERR_OOM
@@ -170,15 +191,21 @@ def test_cancel_and_close(ctx):
         srv.cancel(sids[0])
         info = srv.wait(sids[0])
         assert info.status in (jfcut.OK, jfcut.ERR_CANCELLED)
-        for sid in sids[1:]:
-            assert srv.wait(sid).status == 0
+        for sid, (img, seeds, pf, model) in zip(sids[1:], reqs[1:]):
+            i1 = srv.wait(sid)
+            assert i1.status == 0
+            assert i1.flow == cpu_oracle(img, seeds, pf, model)[0]
         # a cancelled session that has a graph can still be edited and re-solved
         img, seeds, pf, model = reqs[0]
         ed = strokes(seeds.shape, 99, 1)
         if info.status == jfcut.ERR_CANCELLED:
             try:
                 srv.edit(sids[0], *ed[0])
-                srv.wait(sids[0])
+                info2 = srv.wait(sids[0])
+                if info2.status == 0:
+                    flow, lab = cpu_oracle(img, seeds, pf, model, ed)
+                    assert info2.flow == flow
+                    assert np.array_equal(srv.labels(sids[0], seeds.shape), lab)
             except jfcut.JfcError as e:
                 assert e.code == jfcut.ERR_STATE    # cancelled before its build
         for sid in sids:

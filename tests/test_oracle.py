@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 import oracle
+import synthetic
 from conftest import FIXTURES, load_fixture, random_grid
 
 MODEL = dict(lambda_n=100, z_weight_pct=100, lambda_t=10, k_fg=2, k_bg=2, seed_cap=1000000, kmeans_iters=32)
@@ -81,8 +82,7 @@ def test_edge_cases():
 
 
 def test_build_model_gray_ellipse():
-    import jfcut
-    img, seeds = jfcut.synth_gray_ellipse(512, 512, seed=7)
+    img, seeds = synthetic.gray_ellipse(512, 512, seed=7)
     e, caps, st = oracle.build_graph(img, seeds, 0, MODEL)
     h, w = img.shape
     c = [x.reshape(h, w) for x in caps]
@@ -100,8 +100,7 @@ def test_build_model_gray_ellipse():
 
 
 def test_no_seeds_rejected():
-    import jfcut
-    img, seeds = jfcut.synth_gray_ellipse(64, 64, seed=1)
+    img, seeds = synthetic.gray_ellipse(64, 64, seed=1)
     seeds[seeds == 2] = 0
     with pytest.raises(ValueError):
         oracle.build_graph(img, seeds, 0, MODEL)
@@ -109,8 +108,7 @@ def test_no_seeds_rejected():
 
 @needs_ref
 def test_gray_ellipse_flow_vs_bk():
-    import jfcut
-    img, seeds = jfcut.synth_gray_ellipse(512, 512, seed=3)
+    img, seeds = synthetic.gray_ellipse(512, 512, seed=3)
     e, caps, st = oracle.build_graph(img, seeds, 0, MODEL)
     fb, labb, _ = oracle.bk_maxflow(img.shape, e, caps)
     f, _, _, lab = oracle.maxflow(img.shape, e, caps)

@@ -227,8 +227,9 @@ def bench_batched(jfcut, torch, ctx, stream, steps, warmup, n_inst=256):
     """Batched workload: n_inst independent 2D 4-conn RGB instances with sides
     drawn uniformly in [128, 2048] (seeded), generated like the plain workload.
     Batched = every instance in one persistent launch per phase (device work
-    queue, CUDA-graph cycles, autotuned schedule); plain = the same graphs
-    solved one after another with the same schedule.  Both time the solve only
+    queue, CUDA-graph cycles, the schedule the autotuner chose for the batch);
+    plain = the same graphs solved one after another by the plain solver with
+    its default schedule.  Both time the solve only
     (capacity build untimed between steps: it is the same per-instance work in
     both); every flow and cut of the batch must equal the plain ones."""
     rng = np.random.default_rng(SEED + 256)
@@ -368,20 +369,29 @@ def bench_fastcut(jfcut, torch, w=4096, h=3072, reps=2):
     return out
 
 
-def bench_serve(jfcut, torch, ctx, n_req=48, rate=200.0, budget_gb=96):
-    """Serving workload: Poisson arrivals (mean `rate`/s) of n_req sessions,
-    70% 2D RGB images (sides U[256,4096], 4-conn) and 30% int16 phantom
-    volumes (sides U[128,512], 6-conn, N(0,10) noise); each session then sends
-    1-5 stroke edits (0.1-2% of its nodes) one after another, re-solved warm
-    on the device-resident residual graph.  Latency is per request, client
-    side of the C ABI (submit -> result); throughput is all solved nodes over
-    the wall time of the run.  Each session's final flow is checked against a
-    cold plain solve of the same edited graph."""
+def bench_serve(jfcut, torch, ctx, seconds=20.0, rate=200.0, budget_gb=96, max_cold_outstanding=64,
+                pool_2d=16, pool_3d=8, baseline_samples=8):
+    """Serving workload: `seconds` of Poisson arrivals (mean `rate`/s), each a
+    new session: 70% 2D RGB images (sides U[256,4096], 4-conn), 30% int16
+    sphere-and-tube phantom volumes (sides U[128,512], 6-conn, N(0,10)
+    noise); after its cold result a session sends 1-5 stroke edits (0.1-2%
+    of its nodes) one after another, each re-solved warm on the
+    device-resident residual graph, then closes.  Inputs come from a seeded
+    pool (pool_2d images, pool_3d volumes, 5 strokes each).
+
+    The offered load is several times what one GPU solves, so the client
+    sheds: an arrival that finds max_cold_outstanding cold requests
+    unfinished is rejected (counted, never submitted), which bounds the
+    admission queue the way a front end returning "busy" would.  Reported:
+    offered vs served load, shed fraction, p50/p99 latency (client side of the
+    C ABI, submit -> result) per class (cold / warm x 2D / volume), and a
+    baseline of cold plain re-solves (build + the session's edits + solve on
+    the idle GPU) of sampled sessions, whose flows must equal the served
+    ones."""
     rng = np.random.default_rng(SEED + 200)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
-    sess = []
-    for i in range(n_req):
-        if rng.random() < 0.7:
+    pool = []
+    for i in range(pool_2d + pool_3d):
+        if i < pool_2d:
             w, h = (int(v) for v in rng.integers(256, 4097, 2))
             img, seeds = make_workload(w, h, SEED + 9000 + i)
             pf = jfcut.PIX_RGB8
@@ -390,64 +400,104 @@ def bench_serve(jfcut, torch, ctx, n_req=48, rate=200.0, budget_gb=96):
             img, seeds = synthetic.i16_phantom(w, h, d, seed=SEED + 9000 + i, noise_sigma=10)
             pf = jfcut.PIX_I16
         n = seeds.size
-        edits = []
-        for k in range(int(rng.integers(1, 6))):
+        strokes = []
+        for k in range(5):
             m = max(1, int(n * rng.uniform(0.001, 0.02)))
-            edits.append(synthetic.stroke(seeds.shape, seed=SEED + 100 * i + k, n=m, label=1 + (k % 2)))
-        sess.append(dict(img=img, seeds=seeds, pf=pf, edits=edits, n=n, dims=seeds.ndim))
+            strokes.append(synthetic.stroke(seeds.shape, seed=SEED + 100 * i + k, n=m, label=1 + (k % 2)))
+        pool.append(dict(img=img, seeds=seeds, pf=pf, strokes=strokes, n=n, dims=seeds.ndim))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, int(rate * seconds * 1.5) + 16))
+    arrivals = arrivals[arrivals < seconds]
+    picks = [(int(rng.integers(0, pool_2d)) if rng.random() < 0.7 else pool_2d + int(rng.integers(0, pool_3d)),
+              int(rng.integers(1, 6))) for _ in arrivals]
     srv = jfcut.Server(ctx, int(budget_gb * (1 << 30)), max_slots=64)
-    records = []
     lock = threading.Lock()
-    t_start = time.perf_counter()
+    records, served, failures = [], [], []
+    state = {"cold_out": 0, "shed": 0, "offered_nodes": 0}
 
-    def client(i):
-        s = sess[i]
-        delay = arrivals[i] - (time.perf_counter() - t_start)
+    def session(j, p, k):
+        s = pool[p]
+        try:
+            sid = srv.submit(s["img"], s["seeds"], s["pf"], MODEL)
+            info = srv.wait(sid, 300000)
+            with lock:
+                state["cold_out"] -= 1
+            rec = [("cold", s["dims"], s["n"], info.ms_total, info.status)]
+            flow = info.flow
+            for idx, ns in s["strokes"][:k]:
+                if info.status:
+                    break
+                srv.edit(sid, idx, ns)
+                info = srv.wait(sid, 300000)
+                rec.append(("warm", s["dims"], s["n"], info.ms_total, info.status))
+                flow = info.flow
+            srv.close_session(sid)
+            with lock:
+                records.extend(rec)
+                if info.status == 0:
+                    served.append((p, k, flow, rec[-1][3]))
+        except Exception as ex:   # reported, the run goes on
+            with lock:
+                failures.append("%s: %s" % (type(ex).__name__, ex))
+
+    threads = []
+    t_start = time.perf_counter()
+    for j, (t_arr, (p, k)) in enumerate(zip(arrivals, picks)):
+        delay = t_arr - (time.perf_counter() - t_start)
         if delay > 0:
             time.sleep(delay)
-        sid = srv.submit(s["img"], s["seeds"], s["pf"], MODEL)
-        info = srv.wait(sid)
-        rec = [("cold", s["n"], s["dims"], info.ms_total, info.status)]
-        for idx, ns in s["edits"]:
-            srv.edit(sid, idx, ns)
-            info = srv.wait(sid)
-            rec.append(("warm", s["n"], s["dims"], info.ms_total, info.status))
-        s["sid"], s["flow"] = sid, info.flow
         with lock:
-            records.extend(rec)
-
-    threads = [threading.Thread(target=client, args=(i,)) for i in range(n_req)]
-    for t in threads:
-        t.start()
-    for t in threads:
-        t.join()
+            state["offered_nodes"] += pool[p]["n"]
+            if state["cold_out"] >= max_cold_outstanding:
+                state["shed"] += 1
+                continue
+            state["cold_out"] += 1
+        th = threading.Thread(target=session, args=(j, p, k))
+        th.start()
+        threads.append(th)
+    t_arrivals = time.perf_counter() - t_start
+    for th in threads:
+        th.join()
     wall = time.perf_counter() - t_start
     sstats = srv.stats()
-    # bit-exactness: every session's final flow equals a cold plain solve of
-    # the same edited graph; labels compared on every 4th session
-    exact = True
-    for j, s in enumerate(sess):
+    srv.close()
+    # baseline: cold plain re-solves of sampled served sessions on the idle
+    # GPU (build + the same edits + solve), flows equal to the served ones
+    base_ms, exact = [], True
+    picked = served[:: max(1, len(served) // baseline_samples)][:baseline_samples]
+    for p, k, flow, warm_ms in picked:
+        s = pool[p]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         g = jfcut.Graph(ctx, s["seeds"].shape)
         g.build_from_image(s["img"], s["seeds"], s["pf"], MODEL)
-        for idx, ns in s["edits"]:
+        for idx, ns in s["strokes"][:k]:
             g.edit_seeds(idx, ns)
         g.solve()
-        exact &= g.flow() == s["flow"]
-        if j % 4 == 0:
-            exact &= bool(np.array_equal(g.labels(), srv.labels(s["sid"], s["seeds"].shape)))
+        base_ms.append((time.perf_counter() - t0) * 1e3)
+        exact &= g.flow() == flow
         g.close()
-        srv.close_session(s["sid"])
-    srv.close()
-    ok = all(r[4] == 0 for r in records)
-    cold = [r[3] for r in records if r[0] == "cold"]
-    warm = [r[3] for r in records if r[0] == "warm"]
-    nodes = sum(r[1] for r in records)
-    return {"workload": "Poisson %.0f req/s, %d sessions (70%% 2D RGB 256-4096 sides, 30%% int16 volumes "
-                        "128-512 sides), 1-5 warm stroke edits each (0.1-2%% of nodes)" % (rate, n_req),
-            "requests": len(records), "all_ok": ok, "bit_exact_vs_cold_plain": bool(exact),
-            "cold_p50_ms": pct(cold, 50), "cold_p99_ms": pct(cold, 99),
-            "warm_p50_ms": pct(warm, 50), "warm_p99_ms": pct(warm, 99),
-            "throughput_mnodes_s": nodes / wall / 1e6, "wall_s": wall,
+
+    def lat(kind, dims):
+        v = [r[3] for r in records if r[0] == kind and r[1] == dims and r[4] == 0]
+        return {"n": len(v), "p50_ms": pct(v, 50), "p99_ms": pct(v, 99)}
+
+    ok = [r for r in records if r[4] == 0]
+    served_nodes = sum(r[2] for r in ok)
+    cold_nodes = sum(r[2] for r in ok if r[0] == "cold")
+    return {"workload": "Poisson %.0f req/s for %.0f s: new sessions of 70%% 2D RGB (sides 256-4096) and 30%% int16 "
+                        "phantom volumes (sides 128-512), 1-5 warm stroke edits each (0.1-2%% of nodes); arrivals "
+                        "finding %d cold requests unfinished are shed" % (rate, seconds, max_cold_outstanding),
+            "arrivals": int(len(arrivals)), "shed": state["shed"], "sessions_served": len(served),
+            "requests_ok": len(ok), "requests_failed": len(records) - len(ok) + len(failures),
+            "failures": failures[:3],
+            "offered_gnodes_s": state["offered_nodes"] / seconds / 1e9,
+            "served_cold_gnodes_s": cold_nodes / wall / 1e9,
+            "served_all_gnodes_s": served_nodes / wall / 1e9,
+            "latency": {"cold_2d": lat("cold", 2), "cold_3d": lat("cold", 3),
+                        "warm_2d": lat("warm", 2), "warm_3d": lat("warm", 3)},
+            "cold_resolve_baseline": {"samples": len(base_ms), "p50_ms": pct(base_ms, 50),
+                                      "bit_exact_vs_served": bool(exact)},
+            "wall_s": wall, "arrival_window_s": t_arrivals,
             "budget_gb": budget_gb, "peak_used_gb": sstats["peak_used"] / 2**30,
             "peak_solving": sstats["peak_solving"], "loops": sstats["loops"]}
 
@@ -506,7 +556,7 @@ def main():
     ap.add_argument("--extras", default="video,batched,edit4096,serve,fastcut",
                     help="comma list of extra sections at N=1 (video, batched, edit4096, serve, fastcut) "
                          "or 'none'")
-    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--serve-seconds", type=float, default=20.0, help="arrival window of the serve section")
     ap.add_argument("--video-size", default="2560x1440x50", help="WxHxD of the video section")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -645,7 +695,7 @@ def main():
                     "batched": lambda: bench_batched(jfcut, torch, ctx, stream, 2, 1),
                     "edit4096": lambda: bench_edit4096(jfcut, torch, ctx),
                     "fastcut": lambda: bench_fastcut(jfcut, torch),
-                    "serve": lambda: bench_serve(jfcut, torch, ctx, n_req=args.serve_requests)}
+                    "serve": lambda: bench_serve(jfcut, torch, ctx, seconds=args.serve_seconds)}
         with torch.cuda.stream(stream):
             for name in ("video", "batched", "edit4096", "serve", "fastcut"):
                 if name in extras:

@@ -92,6 +92,16 @@ typedef struct jfc_params {
                             (graphcut_push_relabel_fast.cl), for comparison; plain solves only,
                             relabel_interval iterations between global relabels; 2: block-wise
                             on whole 32 x 16 tiles */
+  int spin_limit;        /* polls before a device-side wait gives up (grid barrier, relabel
+                            worklist): 0 = default (2^26 polls, seconds); on expiry the
+                            kernels leave, the call returns JFC_ERR_CUDA ("timed out") and the
+                            context stays usable */
+  int relabel_cap;       /* distance cap of the global relabels while solving: nodes farther
+                            than this from every deficit count as unreachable until no active
+                            tile is left, then one exact (uncapped) relabel certifies the maximum
+                            preflow and the solve goes on uncapped if it finds reachable excess;
+                            flow and cut are those of the exact solve.  0 = automatic, < 0 = no
+                            cap (every relabel exact) */
 } jfc_params;
 
 /* Capacity model (replaces computeCapacity / kmeans / computeExcessFlowLazy,
@@ -204,19 +214,20 @@ int jfc_graph_edit_seeds(jfc_graph* g, const uint32_t* idx, const uint8_t* new_s
 
 /* Solve a 2D 4-connected grid without allocating anything.  No counterpart in
  * the reference: it exists for callers that cannot allocate device memory
- * when they need a cut (code running during CUDA stream capture, real-time
- * frame loops that must not stall on the allocator, hosts with a fixed memory
- * budget).  The working set lives in one fixed file-scope device array of
- * about 13.2 MB that every GPU loading the library holds until exit; grids
- * are limited to 524,288 nodes after padding (width to a multiple of 32,
- * height to a multiple of 16), larger ones return JFC_ERR_INVALID_ARG.
+ * when they need a cut (real-time frame loops that must not stall on the
+ * allocator, hosts that hand the library a fixed memory budget up front).
+ * The working set lives in one fixed file-scope device array of about
+ * 13.2 MB that every GPU loading the library holds until exit; grids are
+ * limited to 524,288 nodes after padding (width to a multiple of 32, height
+ * to a multiple of 16), larger ones return JFC_ERR_INVALID_ARG.
  * Inputs d_excess and d_ncap[4] (reference channel order, dense w*h int32)
  * and the output d_labels (w*h bytes, 1 = source side) are caller-owned
  * device buffers on `device`; *flow receives the int64 max-flow.  stream is
- * a cudaStream_t (NULL = the legacy default stream); params may be NULL.
- * Calls share the array: calls that overlap on the GPU race.  The first call
- * on a device looks up the array's address; make it before any stream
- * capture begins. */
+ * a cudaStream_t (NULL = the legacy default stream); the call synchronises
+ * it before returning (counters are read back between relabel cycles) and
+ * restores the caller's current device.  params may be NULL.  Calls share
+ * the array: calls that overlap on the GPU race.  The first call on a device
+ * looks up the array's address; make it before any stream capture begins. */
 int jfc_solve_grid2d_noalloc(int device, void* stream, const jfc_params* params, int w, int h,
                              const int32_t* d_excess, const int32_t* const* d_ncap,
                              int64_t flow_offset, uint8_t* d_labels, int64_t* flow);
@@ -230,10 +241,14 @@ int  jfc_batch_add(jfc_batch* b, jfc_graph* g);     /* graph must be built/set *
 int  jfc_batch_clear(jfc_batch* b);
 int  jfc_batch_size(jfc_batch* b);
 /* Solve every graph of the batch; stats may be NULL or an array of the
- * batch's size.  Returns the first non-OK per-graph status. */
+ * batch's size.  Returns the first non-OK per-graph status.  The schedule is
+ * the one jfc_batch_autotune chose for this batch, else the context's. */
 int  jfc_batch_solve(jfc_batch* b, jfc_stats* stats);
-/* Pick tile_rows / local_iters / relabel_interval for this batch by timing
- * candidates on a copy of the batch's graphs (state is restored). */
+/* Pick tile_rows / local_iters / relabel_interval (and 3D tile depth) for
+ * this batch by timing candidates on a copy of the batch's graphs (state is
+ * restored; each candidate is the faster of two solves).  The choice is
+ * written to *chosen (may be NULL) and applies to this batch's later solves;
+ * the context's parameters are left unchanged.  jfc_batch_clear drops it. */
 int  jfc_batch_autotune(jfc_batch* b, jfc_params* chosen);
 
 /* ---- serving: continuous batching with HBM-budget admission and warm

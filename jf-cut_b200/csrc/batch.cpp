@@ -8,7 +8,8 @@
 // from the device work queue, and the host loop runs once for the whole batch
 // (converged grids simply stop producing flagged tiles).  The autotuner times
 // candidate schedules (tile height, rounds per visit, relabel interval) on the
-// batch itself and restores the graphs' state after each trial.
+// batch itself and restores the graphs' state after each trial; its choice
+// belongs to the batch (the context's parameters stay as the caller set them).
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -22,16 +23,22 @@ struct jfc_batch {
   TileSet ts[2];          // [0] 2D grids, [1] 3D grids
   int shape[2] = {-1, -1};
   bool dirty = true;
+  bool tuned = false;     // params below were chosen by jfc_batch_autotune
+  jfc_params params{};
 };
 
 namespace {
 
+// The schedule this batch solves with: its tuned one, else the context's.
+const jfc_params& batch_params(const jfc_batch* b) { return b->tuned ? b->params : b->ctx->params; }
+
 int rebuild(jfc_batch* b) {
-  const int tr = b->ctx->params.tile_rows;
+  const jfc_params& bp = batch_params(b);
+  const int tr = bp.tile_rows;
   for (int k = 0; k < 2; ++k) {
     const int dims = k ? 3 : 2;
-    const int td = b->ctx->params.tile_depth;
-    const bool split = pr_split_for(b->ctx->params, dims);
+    const int td = bp.tile_depth;
+    const bool split = pr_split_for(bp, dims);
     const int code = shape_code(dims, tr, td, split);
     if (!b->dirty && b->shape[k] == code) continue;
     std::vector<GridDev> v;
@@ -109,6 +116,7 @@ int jfc_batch_clear(jfc_batch* b) {
   if (!b) return set_error(JFC_ERR_INVALID_ARG, "null batch");
   b->graphs.clear();
   b->dirty = true;
+  b->tuned = false;       // a schedule tuned for the old graphs does not carry over
   return JFC_OK;
 }
 
@@ -127,7 +135,7 @@ int jfc_batch_solve(jfc_batch* b, jfc_stats* stats) {
     const int dims = k ? 3 : 2;
     std::vector<GridResult> res;
     jfc_stats st;
-    rc = engine_solve(b->ctx, b->ts[k], b->ctx->params, res, st);
+    rc = engine_solve(b->ctx, b->ts[k], batch_params(b), res, st);
     if (rc && rc != JFC_ERR_NOT_CONVERGED) return rc;
     int gi = 0;
     for (size_t i = 0; i < b->graphs.size(); ++i) {
@@ -156,19 +164,34 @@ int jfc_batch_autotune(jfc_batch* b, jfc_params* chosen) {
   Snapshot snap;
   int rc = snapshot(b, snap, false);
   if (rc) return rc;
-  const jfc_params base = b->ctx->params;
-  // one timed solve of the batch from the snapshot under schedule p
+  const bool was_tuned = b->tuned;
+  const jfc_params was = b->params;
+  const jfc_params base = batch_params(b);
+  auto give_up = [&](int r) { b->tuned = was_tuned; b->params = was; b->dirty = true; return r; };
+  // a trial: the batch solved from the snapshot under schedule p, twice; its
+  // time is the faster of the two device-clock solve times (one sample can
+  // be slowed by anything else on the host or device)
+  std::vector<jfc_stats> st(b->graphs.size());
   auto trial = [&](const jfc_params& p, double& ms) -> int {
-    b->ctx->params = p;
-    b->ctx->params.relabel_interval_max = 0;   // re-derived from the trial interval
-    fill_defaults(b->ctx->params);
-    int r = snapshot(b, snap, true);
-    if (r) return r;
-    const auto t0 = std::chrono::steady_clock::now();
-    r = jfc_batch_solve(b, nullptr);
-    const auto t1 = std::chrono::steady_clock::now();
-    ms = r ? 1e30 : std::chrono::duration<double, std::milli>(t1 - t0).count();
-    return r == JFC_ERR_NOT_CONVERGED ? JFC_OK : r;
+    b->params = p;
+    b->params.relabel_interval_max = 0;   // re-derived from the trial interval
+    fill_defaults(b->params);
+    b->tuned = true;
+    ms = 1e30;
+    for (int rep = 0; rep < 2; ++rep) {
+      int r = snapshot(b, snap, true);
+      if (r) return r;
+      r = jfc_batch_solve(b, st.data());
+      if (r == JFC_ERR_NOT_CONVERGED) return JFC_OK;   // this schedule ran out of budget: not chosen
+      if (r) return r;
+      // the batch's solves are one engine run per dimensionality; each
+      // graph's stats carry the time of the run it was part of
+      double t2 = 0.0, t3 = 0.0;
+      for (size_t i = 0; i < b->graphs.size(); ++i)
+        (b->graphs[i]->dims == 2 ? t2 : t3) = st[i].ms_total;
+      ms = std::min(ms, t2 + t3);
+    }
+    return JFC_OK;
   };
   // Coordinate descent from the context's schedule: relabel interval, then
   // rounds per visit, then tile height (then 3D tile depth when the batch has
@@ -178,9 +201,9 @@ int jfc_batch_autotune(jfc_batch* b, jfc_params* chosen) {
   jfc_params best = base;
   double best_ms = 1e30, ms = 0.0;
   rc = trial(best, ms);
-  if (rc) { b->ctx->params = base; return rc; }
+  if (rc) return give_up(rc);
   rc = trial(best, best_ms);
-  if (rc) { b->ctx->params = base; return rc; }
+  if (rc) return give_up(rc);
   const int intervals[] = {2, 3, 4, 8, 16};
   const int iters[] = {8, 12, 16, 32};
   const int rows[] = {8, 16};
@@ -198,13 +221,14 @@ int jfc_batch_autotune(jfc_batch* b, jfc_params* chosen) {
       if (field == vals[i]) continue;
       field = vals[i];
       rc = trial(p, ms);
-      if (rc) { b->ctx->params = base; return rc; }
+      if (rc) return give_up(rc);
       if (ms < best_ms) { best_ms = ms; best = p; }
     }
   }
   best.relabel_interval_max = 0;
   fill_defaults(best);
-  b->ctx->params = best;
+  b->params = best;
+  b->tuned = true;
   rc = snapshot(b, snap, true);
   for (jfc_graph* g : b->graphs) g->state = 1;
   if (chosen) *chosen = best;

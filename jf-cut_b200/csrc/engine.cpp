@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -67,6 +68,7 @@ void fill_defaults(jfc_params& p) {
     p.relabel_interval_max = std::max(64, 16 * p.relabel_interval);
   if (p.max_sweeps <= 0) p.max_sweeps = 1 << 20;
   if (p.max_bfs_passes <= 0) p.max_bfs_passes = 1 << 20;
+  if (p.spin_limit < 0) p.spin_limit = 0;   // 0: the device default (2^26 polls)
 }
 
 double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
@@ -234,8 +236,9 @@ static size_t pin_need(const TileSet& ts) {
   return sizeof(DevCounters) + sizeof(long long) * 2 * (size_t)ts.ngrids + 64;
 }
 
-// pinned slot holding the sweep pairs of the next push-relabel phase (after
-// the read-back area); copied to the control block by the cycle itself
+// pinned slot holding the sweep pairs of the next push-relabel phase and the
+// distance cap of the relabel after it (after the read-back area); copied to
+// the control block (pr_sweeps, h_cap) by the cycle itself
 static int* pin_sweeps(jfc_ctx* ctx, const TileSet& ts) {
   return (int*)((char*)ctx->h_pin + (pin_need(ts) + 255) / 256 * 256);
 }
@@ -322,7 +325,9 @@ void tileset_drop_graphs(TileSet& ts) {
 static cudaError_t enqueue_cycle(TileSet& ts, const int* pin_sw, int local_iters, int max_passes, cudaStream_t s,
                                  void* pin) {
   cudaError_t e = cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&ts.d_ctr->pr_sweeps, pin_sw, sizeof(int), cudaMemcpyHostToDevice, s);
+  static_assert(offsetof(DevCounters, h_cap) == offsetof(DevCounters, pr_sweeps) + sizeof(int),
+                "pr_sweeps and h_cap are copied together");
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&ts.d_ctr->pr_sweeps, pin_sw, 2 * sizeof(int), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = launch_pr_phase(ts, 0, local_iters, s);
   if (e == cudaSuccess) e = enqueue_bfs(ts, false, max_passes, s, pin);
   return e;
@@ -367,13 +372,14 @@ static cudaGraphExec_t cycle_graph(TileSet& ts, const int* pin_sw, int local_ite
 
 // One relabel cycle, replayed from a graph when enabled; returns the outcome
 // of its global relabel.
-static int run_cycle(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, int interval, int& passes,
+static int run_cycle(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, int interval, int h_cap, int& passes,
                      std::vector<int>& active, int* sweeps_done, bool* used_graph) {
   cudaStream_t s = ctx->stream;
   int rc = pin_reserve(ctx, pin_need_cycle(ts));
   if (rc) return rc;
   int* pin_sw = pin_sweeps(ctx, ts);
-  *pin_sw = interval;   // the previous cycle's copies finished at its sync
+  pin_sw[0] = interval;   // the previous cycle's copies finished at its sync
+  pin_sw[1] = h_cap;
   cudaGraphExec_t x = p.use_graph ? cycle_graph(ts, pin_sw, p.local_iters, p.max_bfs_passes, s, ctx->h_pin)
                                   : nullptr;
   if (x) {
@@ -425,6 +431,11 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   } ev_free{ev};
   JFC_CUDA(cudaEventRecord(ev[0], s));
   JFC_CUDA(launch_clear_counters(ts, s));
+  // capped relabels while solving (the first one included), then one exact
+  // relabel certifies the result
+  int h_cap = relabel_cap_for(p, ts.dims);
+  if (p.spin_limit > 0 || h_cap > 0)
+    JFC_CUDA(launch_set_limits(ts, (unsigned long long)p.spin_limit, h_cap, s));
 #ifndef JFC_NO_PREPUSH
   if (p.pr_mode != 1) JFC_CUDA(launch_prepush(ts, s));   // the Fast-Cut comparison stays as it was
 #endif
@@ -457,6 +468,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
     last_pr = c0->ns_pr;
     last_gr = c0->ns_gr_first + c0->ns_gr_frontier;
   }
+  for (;;) {
   while (total() > 0) {
     if (st.sweeps >= p.max_sweeps) {
       status = set_error(JFC_ERR_NOT_CONVERGED, "sweep budget exhausted");
@@ -479,7 +491,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
       last_pr -= (unsigned long long)(fms * 1e6);   // the cost rule below sees the sweeps' time
       sw = 2 * interval;
     } else {
-      rc = run_cycle(ctx, ts, p, interval, st.bfs_passes, active, &sw, &graphs);
+      rc = run_cycle(ctx, ts, p, interval, h_cap, st.bfs_passes, active, &sw, &graphs);
       if (rc) return rc;
     }
     st.sweeps += sw;
@@ -502,6 +514,19 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
       prev_pr = pr;
       prev_gr = gr;
     }
+  }
+  // no active tile under the cap: one exact relabel decides.  Excess it finds
+  // reachable (farther than the cap from every deficit) keeps the solve going
+  // with exact relabels; none means the preflow is maximum.
+  if (status != JFC_OK || h_cap == 0) break;
+  h_cap = 0;
+  JFC_CUDA(launch_set_limits(ts, (unsigned long long)p.spin_limit, 0, s));
+  rc = engine_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, nullptr);
+  if (rc) return rc;
+  ++st.global_relabels;
+  if (p.verbose)
+    fprintf(stderr, "{\"relabel\": %d, \"exact\": true, \"active_tiles\": %lld}\n", st.global_relabels, total());
+  if (total() == 0) break;
   }
   if (status != JFC_OK) {
     for (int g = 0; g < ts.ngrids; ++g)

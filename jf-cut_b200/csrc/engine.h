@@ -85,6 +85,13 @@ bool pr_split_for(const jfc_params& p, int dims);
 inline int interval_for(const jfc_params& p, int dims) {
   return p.relabel_interval > 0 ? p.relabel_interval : (dims == 2 ? 2 : 3);
 }
+// Distance cap of the global relabels while solving (0: none): relabel_cap,
+// or when it is 0 the measured default per dimensionality.  The Fast-Cut
+// comparison mode keeps the reference's exact relabels.
+inline int relabel_cap_for(const jfc_params& p, int dims) {
+  if (p.pr_mode == 1 || p.relabel_cap < 0) return 0;
+  return p.relabel_cap > 0 ? p.relabel_cap : (dims == 2 ? 64 : 32);
+}
 
 int set_error(int code, const std::string& msg);
 int cuda_status(cudaError_t e, const char* where);

@@ -52,6 +52,8 @@ struct DevCounters {
   int bfs_status;            // 1 converged, 2 pass budget exhausted
   int sweeps_done;           // sweeps run by the last push-relabel phase
   int pr_sweeps;             // sweep pairs of the next phase when launched with sweeps <= 0
+  int h_cap;                 // global relabels: distances >= h_cap count as unreachable (0: no cap);
+                             // adjacent to pr_sweeps: a relabel cycle copies both at once
   int fast_moved;            // a Fast-Cut push moved flow (comparison mode)
   unsigned long long visits; // push-relabel tile visits
   unsigned long long bfs_visits;
@@ -61,6 +63,7 @@ struct DevCounters {
   unsigned long long ns_pr;           // push-relabel phases, device ns
   unsigned long long t_gr_start;      // device clock at the start of the last relabel
   unsigned long long prof[8];         // SM-cycle split of push-relabel visits (JFC_PHASE_CLOCK builds)
+  unsigned long long spin_limit;  // polls before a device-side wait gives up (0: 2^26)
   unsigned wl_head;          // 2D relabel worklist: tickets taken
   unsigned wl_tail;          // 2D relabel worklist: ring positions reserved
   int wl_out;                // 2D relabel worklist: items queued and not yet fully visited
@@ -129,7 +132,13 @@ cudaError_t launch_bfs(const TileSet& ts, bool cut, int max_passes, cudaStream_t
 cudaError_t launch_tag(const TileSet& ts, const uint8_t* d_seeds, int max_passes, cudaStream_t s);
 cudaError_t launch_grid_sums(const TileSet& ts, cudaStream_t s);
 cudaError_t launch_clear_counters(const TileSet& ts, cudaStream_t s);
+// Polls before the device-side waits of later launches give up (0: default)
+// and the distance cap of the global relabels (0: none).
+cudaError_t launch_set_limits(const TileSet& ts, unsigned long long polls, int h_cap, cudaStream_t s);
 int persistent_blocks(const void* kernel, int threads, size_t smem);
+// persistent_blocks on the current device, cached per device in cache[64]
+// (every cooperative launch of one kernel reuses its grid size)
+int persistent_blocks_cached(int* cache, const void* kernel, int threads);
 // layout helpers (kernels_bfs.cu)
 cudaError_t launch_fix_boundary(const GridDev& g, int conn, int* d_bad, cudaStream_t s);
 cudaError_t launch_pack_labels(const GridDev& g, uint8_t* d_dense, cudaStream_t s);

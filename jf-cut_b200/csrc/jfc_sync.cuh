@@ -8,10 +8,17 @@ namespace jfc {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// Polls a device-side wait makes before it gives up: ctr->spin_limit, or
+// 2^26 (seconds) when it is 0.
+__device__ __forceinline__ unsigned long long spin_cap(const DevCounters* ctr) {
+  const unsigned long long v = *(const volatile unsigned long long*)&ctr->spin_limit;
+  return v ? v : (1ull << 26);
+}
+
 // Grid-wide barrier of a cooperative launch.  Every wait is bounded: after
-// ~2^26 polls (seconds) the barrier raises ctr->error and returns false, and
-// every block leaves its loop on the next check, so a lost block can never
-// hang the device.  `on_last` runs on the last block to arrive, before the
+// spin_cap polls the barrier raises ctr->error and returns false, and every
+// block leaves its loop on the next check, so a lost block can never hang
+// the device.  `on_last` runs on the last block to arrive, before the
 // release (queue / ticket resets between phases).
 template <typename F>
 __device__ __forceinline__ bool grid_sync(DevCounters* ctr, F on_last) {
@@ -30,9 +37,10 @@ __device__ __forceinline__ bool grid_sync(DevCounters* ctr, F on_last) {
       atomicAdd(&ctr->bar_gen, 1u);
     } else {
       unsigned long long spins = 0;
+      const unsigned long long cap = spin_cap(ctr);
       while (*vgen == g) {
         if (*verr) { ok = 0; break; }
-        if (++spins > (1ull << 26)) { atomicExch(&ctr->error, 1); ok = 0; break; }
+        if (++spins > cap) { atomicExch(&ctr->error, 1); ok = 0; break; }
         __nanosleep(100);
       }
     }
@@ -44,6 +52,13 @@ __device__ __forceinline__ bool grid_sync(DevCounters* ctr, F on_last) {
 }
 
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
+
+// Distance cap of the running global relabel: distances at or above it are
+// stored as unreachable (JFC_INF); no cap when ctr->h_cap is 0.
+__device__ __forceinline__ int height_cap(const DevCounters* ctr) {
+  const int v = vload(&ctr->h_cap);
+  return v > 0 ? v : JFC_INF;
+}
 
 // Device-wide nanosecond clock (phase timing of the persistent kernels).
 __device__ __forceinline__ unsigned long long global_ns() {

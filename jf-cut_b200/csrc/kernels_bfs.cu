@@ -48,13 +48,14 @@ struct RlRing {
   unsigned* tail;
   int* out;
   int* err;
+  unsigned long long max_spins;   // polls before a wait gives up
 };
 
 // Append the tiles offered by the lanes of a warp that win their queued
 // flag: count them as outstanding first (so the count never reaches zero
 // while one is on its way), then reserve ring positions and claim each slot
-// (free, or freed by its reader within a few polls; bounded: after ~2^26
-// polls the error flag is raised).  Returns false after an error.
+// (free, or freed by its reader within a few polls; bounded: after
+// W.max_spins polls the error flag is raised).  Returns false after an error.
 __device__ __forceinline__ bool ring_append(bool want, int tile, int* flags, const RlRing& W) {
   bool won = false;
   if (want) won = atomicExch(flags + tile, 1) == 0;
@@ -73,7 +74,7 @@ __device__ __forceinline__ bool ring_append(bool want, int tile, int* flags, con
     __threadfence();
     unsigned long long spins = 0;
     while (atomicCAS(slot, -1, tile) != -1) {
-      if (++spins > (1ull << 26) || *(volatile int*)W.err) { atomicExch(W.err, 1); ok = false; break; }
+      if (++spins > W.max_spins || *(volatile int*)W.err) { atomicExch(W.err, 1); ok = false; break; }
       __nanosleep(64);
     }
   }
@@ -488,9 +489,12 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
     if (arcs & jfc::A_ZP) m = min(m, s.h[hi + T::SZ]);
     if (arcs & jfc::A_ZM) m = min(m, s.h[hi - T::SZ]);
   }
-  const bool need = __syncthreads_or(m + 1 < hstart);
+  const int cap = jfc::height_cap(ts.d_ctr);
+  const bool need = __syncthreads_or(m + 1 < hstart && m + 1 < cap);
   const bool converged = need ? jfc::relax_cta<DIMS, TY, TZ>(s.h, s.arc, 16) : true;
-  const int hf = s.h[hi];
+  // distances at or above the cap stay unreachable (every stored height is
+  // below the cap or JFC_INF, so the capped closure is the closure clamped)
+  const int hf = s.h[hi] < cap ? s.h[hi] : hstart;
   const bool changed = hf != hstart;
   if (changed) {
     g.h[n] = hf;
@@ -630,7 +634,9 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
 #pragma unroll
   for (int i = 0; i < R; ++i) h[i] = ((DEF[i] >> lane) & 1u) ? 0 : JFC_INF;
   // level-synchronous expansion: u reaches level d+1 through an arc to a level-d node
-  for (int d = 0; d < 32 * R; ++d) {
+  // (levels at or above the relabel's distance cap stay unreachable)
+  const int dmax = min(32 * R, jfc::height_cap(ts.d_ctr) - 1);
+  for (int d = 0; d < dmax; ++d) {
     unsigned any = 0;
     unsigned N[R];
 #pragma unroll
@@ -771,8 +777,9 @@ __device__ __forceinline__ void relabel_frontier_warp(const TileSet& ts, int tid
   for (int i = 0; i < R; ++i) F[i] = 0u;
   unsigned rows_changed = 0, c0 = 0, c31 = 0;
   bool again = false;
+  const int cap = jfc::height_cap(ts.d_ctr);   // levels at or above it stay unreachable
   int d = next_level(-1);
-  for (int level = 0; d < JFC_INF; ++level) {
+  for (int level = 0; d < cap; ++level) {
     if (level >= kMaxLevels) { again = true; break; }
     const unsigned sx = __ballot_sync(FULL, HX + 1 == d);
     unsigned N[R];
@@ -969,27 +976,29 @@ __global__ void __launch_bounds__(256) k_relabel_warp(TileSet ts, int max_passes
 // queues the tile for a full visit only when some residual arc u -> v out of
 // the tile has h(v) + 1 < h(u).
 template <int TY>
-__device__ __forceinline__ bool border_improvable(const TileSet& ts, int tid, int lane) {
+__device__ __forceinline__ bool border_improvable(const TileSet& ts, int tid, int lane, int cap) {
   const int4 ti = ts.d_info[tid];
   const GridDev& g = ts.d_desc[ti.x];
   const long long pitch = g.pitch;
   const int x0 = ti.y * 32, y0 = ti.z * TY;
   const long long base = (long long)x0 + (long long)y0 * pitch;
+  // a distance offered through the arc counts only below the relabel's cap
+  auto better = [&](long long n, long long m) { const int v = g.h[m] + 1; return v < g.h[n] && v < cap; };
   bool imp = false;
   if (y0 > 0) {   // top row, arcs -y
     const long long n = base + lane;
-    if ((g.label[n] & jfc::A_YM) && g.h[n - pitch] + 1 < g.h[n]) imp = true;
+    if ((g.label[n] & jfc::A_YM) && better(n, n - pitch)) imp = true;
   }
   if (y0 + TY < g.Hp) {   // bottom row, arcs +y
     const long long n = base + lane + (TY - 1) * pitch;
-    if ((g.label[n] & jfc::A_YP) && g.h[n + pitch] + 1 < g.h[n]) imp = true;
+    if ((g.label[n] & jfc::A_YP) && better(n, n + pitch)) imp = true;
   }
   if (lane < TY && x0 > 0) {   // left column, arcs -x
     const long long n = base + lane * pitch;
-    if ((g.label[n] & jfc::A_XM) && g.h[n - 1] + 1 < g.h[n]) imp = true;
+    if ((g.label[n] & jfc::A_XM) && better(n, n - 1)) imp = true;
   } else if (lane >= 16 && lane < 16 + TY && x0 + 32 < pitch) {   // right column, arcs +x
     const long long n = base + 31 + (lane - 16) * pitch;
-    if ((g.label[n] & jfc::A_XP) && g.h[n + 1] + 1 < g.h[n]) imp = true;
+    if ((g.label[n] & jfc::A_XP) && better(n, n + 1)) imp = true;
   }
   return __any_sync(jfc::FULL, imp);
 }
@@ -1025,7 +1034,7 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
         if ((int)k >= n) break;
         const int tt = queue[k];
         if (lane == 0) fcur[tt] = 0;
-        const bool imp = border_improvable<TY>(ts, tt, lane);
+        const bool imp = border_improvable<TY>(ts, tt, lane, jfc::height_cap(ctr));
         jfc::warp_append(imp && lane == 0, tt, Q.flags, Q.q, Q.qn);
       }
     } else {
@@ -1070,27 +1079,42 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
       busy[i] = 0;
     }
     ok = jfc::grid_sync(ctr, [&]() {});
-    const RlRing W{ring, cap, &ctr->wl_tail, &ctr->wl_out, &ctr->error};
+    const unsigned long long max_spins = jfc::spin_cap(ctr);
+    const RlRing W{ring, cap, &ctr->wl_tail, &ctr->wl_out, &ctr->error, max_spins};
     const BfsQ Q{ts.d_flag_bfs[0], nullptr, nullptr};
     while (ok) {
       if (threadIdx.x == 0) {
         int tile = -1;
         const unsigned k = atomicAdd(&ctr->wl_head, 1u);
         int* slot = ring + k % cap;
+        // bounded: the item arrives, or the work is done, or an error; the
+        // count measures a stall (it restarts whenever the worklist moves:
+        // items appended or finished), not the length of the relabel
         unsigned long long spins = 0;
-        for (;;) {   // bounded: the item arrives, or the work is done, or an error
+        unsigned seen_tail = jfc::vload((const int*)&ctr->wl_tail);
+        int seen_out = jfc::vload(&ctr->wl_out);
+        for (;;) {
           if (*(volatile int*)slot >= 0) {
             const int v = atomicExch(slot, -1);
             if (v >= 0) { tile = v; break; }
           }
-          if (*(volatile int*)&ctr->wl_out == 0 || *(volatile int*)&ctr->error) break;
-          if (++spins > (1ull << 26)) { atomicExch(&ctr->error, 1); break; }
+          const int out = jfc::vload(&ctr->wl_out);
+          if (out == 0 || *(volatile int*)&ctr->error) break;
+          const unsigned tl = (unsigned)jfc::vload((const int*)&ctr->wl_tail);
+          if (out != seen_out || tl != seen_tail) {
+            seen_out = out;
+            seen_tail = tl;
+            spins = 0;
+          } else if (++spins > max_spins) {
+            atomicExch(&ctr->error, 1);
+            break;
+          }
           __nanosleep(32);
         }
         if (tile >= 0) {
           spins = 0;
           while (atomicCAS(busy + tile, 0, 1) != 0) {
-            if (++spins > (1ull << 26) || *(volatile int*)&ctr->error) { atomicExch(&ctr->error, 1); tile = -1; break; }
+            if (++spins > max_spins || *(volatile int*)&ctr->error) { atomicExch(&ctr->error, 1); tile = -1; break; }
             __nanosleep(32);
           }
         }
@@ -1195,8 +1219,8 @@ cudaError_t bfs_t(const TileSet& ts, int max_passes, const uint8_t* seeds, cudaS
   else if constexpr (DIMS == 2) fn = (const void*)k_relabel_cta<DIMS, TY, TZ>;
   else fn = (const void*)k_relabel_warp<DIMS, TY, TZ>;
   const int nt = (CUT || DIMS == 3) ? 256 : RTile<DIMS, TY, TZ>::NT;
-  static int blocks = 0;
-  if (!blocks) blocks = persistent_blocks(fn, nt, 0);
+  static int cache[64] = {0};
+  const int blocks = persistent_blocks_cached(cache, fn, nt);
   if (!CUT) {
     const long long fb = ((long long)ts.ntiles * 32 + 255) / 256;
     jfc_note_launch();
@@ -1212,8 +1236,8 @@ cudaError_t bfs_t(const TileSet& ts, int max_passes, const uint8_t* seeds, cudaS
 
 template <int TY, int TZ>
 cudaError_t sums_t(const TileSet& ts, cudaStream_t s) {
-  static int blocks = 0;
-  if (!blocks) blocks = persistent_blocks((const void*)k_grid_sums<TY, TZ>, 256, 0);
+  static int cache[64] = {0};
+  const int blocks = persistent_blocks_cached(cache, (const void*)k_grid_sums<TY, TZ>, 256);
   jfc_note_launch();
   k_grid_sums<TY, TZ><<<blocks, 256, 0, s>>>(ts.d_desc, ts.d_info, ts.ntiles, ts.d_grid_sum);
   return cudaGetLastError();
@@ -1302,6 +1326,20 @@ int persistent_blocks(const void* kernel, int threads, size_t smem) {
   return sms * per;
 }
 
+int persistent_blocks_cached(int* cache, const void* kernel, int threads) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return persistent_blocks(kernel, threads, 0);
+  // two threads filling one entry at once compute the same value; the
+  // atomic store keeps the write whole
+  int v = __atomic_load_n(cache + dev, __ATOMIC_RELAXED);
+  if (!v) {
+    v = persistent_blocks(kernel, threads, 0);
+    __atomic_store_n(cache + dev, v, __ATOMIC_RELAXED);
+  }
+  return v;
+}
+
 static cudaError_t bfs_dispatch(const TileSet& ts, int mode, int max_passes, const uint8_t* seeds, cudaStream_t s) {
 #define JFC_BFS(D, Y, Z)                                                       \
   (mode == 1 ? bfs_t<D, Y, Z, 1>(ts, max_passes, seeds, s)                     \
@@ -1347,6 +1385,19 @@ cudaError_t launch_grid_sums(const TileSet& ts, cudaStream_t s) {
 
 cudaError_t launch_clear_counters(const TileSet& ts, cudaStream_t s) {
   return cudaMemsetAsync(ts.d_ctr, 0, sizeof(DevCounters), s);
+}
+
+namespace {
+__global__ void k_set_limits(DevCounters* ctr, unsigned long long polls, int h_cap) {
+  ctr->spin_limit = polls;
+  ctr->h_cap = h_cap;
+}
+}  // namespace
+
+cudaError_t launch_set_limits(const TileSet& ts, unsigned long long polls, int h_cap, cudaStream_t s) {
+  jfc_note_launch();
+  k_set_limits<<<1, 1, 0, s>>>(ts.d_ctr, polls, h_cap);
+  return cudaGetLastError();
 }
 
 static int grid_blocks(long long n) {

@@ -333,8 +333,8 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
 template <int DIMS, int TY, int TZ, bool SPLIT = false>
 cudaError_t launch_t(const TileSet& ts, int sweeps, int local_iters, cudaStream_t st) {
   constexpr int NT = Tile<DIMS, TY, TZ>::NT;
-  static int blocks = 0;
-  if (!blocks) blocks = persistent_blocks((const void*)k_pr_phase<DIMS, TY, TZ, SPLIT>, NT, 0);
+  static int cache[64] = {0};
+  const int blocks = persistent_blocks_cached(cache, (const void*)k_pr_phase<DIMS, TY, TZ, SPLIT>, NT);
   TileSet arg = ts;
   void* params[] = {(void*)&arg, (void*)&sweeps, (void*)&local_iters};
   jfc_note_launch();

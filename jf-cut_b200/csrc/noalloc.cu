@@ -1,14 +1,16 @@
 // noalloc.cu — a 2D solve that allocates nothing.
 //
 // Some callers cannot allocate device memory at the moment they need a cut:
-// code running while a CUDA stream is being captured into a graph (cudaMalloc
-// cannot be captured), real-time frame loops that must not stall on the
-// allocator, and hosts that hand this library a fixed memory budget up front.
+// real-time frame loops that must not stall on the allocator (a cudaMalloc
+// can synchronise the device and take milliseconds), and hosts that hand this
+// library a fixed memory budget up front and forbid allocations after it.
 // jfc_solve_grid2d_noalloc serves them: the whole working set of the solve
 // (residual graph, heights, labels, tile tables, work queues, counters) lives
 // in one file-scope device array of fixed size, so the call itself performs no
 // cudaMalloc / cudaFree / cudaMallocHost and uses no allocating library
-// routine.  The caller passes device inputs and outputs.
+// routine.  The caller passes device inputs and outputs.  The call reads a few
+// counters back between relabel cycles, so it synchronises `stream` before it
+// returns.
 //
 // Limits and sharing:
 //  * grids whose padded size (width rounded up to 32, height rounded up to
@@ -22,7 +24,8 @@
 //    on two streams, or from two threads — race and corrupt each other;
 //  * the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress, once per device, with that device current); make
-//    that first call before any stream capture begins.
+//    that first call before any stream capture begins;
+//  * the caller's current device is restored before the call returns.
 #include <cstring>
 #include <mutex>
 
@@ -55,6 +58,13 @@ constexpr size_t kBytes = kOffBad + 256;
 
 std::mutex g_mu;
 void* g_addr[128] = {nullptr};
+
+// Restores the calling thread's current device when the call returns.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() { if (cudaGetDevice(&prev) != cudaSuccess) prev = -1; }
+  ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
 
 // tile t of a single grid: {grid 0, tx, ty, tz 0}
 __global__ void k_na_tile_info(int4* info, int tiles_x, int ntiles) {
@@ -143,6 +153,7 @@ extern "C" int jfc_solve_grid2d_noalloc(int device, void* stream, const jfc_para
   jfc_params p{};
   if (params) p = *params;
   fill_defaults(p);
+  DeviceGuard restore;
   JFC_CUDA(cudaSetDevice(device));
   char* base = nullptr;
   int rc = na_scratch(device, &base);
@@ -213,6 +224,7 @@ extern "C" int jfc_solve_grid2d_noalloc(int device, void* stream, const jfc_para
 
   // ---- solve: global relabel, push-relabel phases, device-side active count
   JFC_CUDA(launch_clear_counters(ts, s));
+  if (p.spin_limit > 0) JFC_CUDA(launch_set_limits(ts, (unsigned long long)p.spin_limit, 0, s));
   int active = 0, sweeps = 0;
   rc = na_bfs(ts, p, false, s, &active, nullptr);
   if (rc) return rc;

@@ -346,6 +346,8 @@ def test_batch_autotune_restores_and_matches(ctx):
         b.add(g)
     p = b.autotune()
     assert p.tile_rows in (8, 16) and p.local_iters in (8, 12, 16, 32) and p.relabel_interval in (0, 2, 3, 4, 8, 16)
+    # the choice belongs to the batch: the context stays on the defaults
+    use_schedule(ctx, "default")
     # the graphs are back in their built state: solving now gives the plain results
     st = b.solve()
     assert all(s.status == 0 for s in st)

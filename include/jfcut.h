@@ -102,6 +102,10 @@ typedef struct jfc_params {
                             preflow and the solve goes on uncapped if it finds reachable excess;
                             flow and cut are those of the exact solve.  0 = automatic, < 0 = no
                             cap (every relabel exact) */
+  int pr_sched;          /* scheduling of the push-relabel visits between two global relabels:
+                            1 = checkerboard parity sweeps with a grid barrier between colours,
+                            2 = an asynchronous worklist with per-tile neighbour exclusion (no
+                            barriers), 0 = automatic.  Same arithmetic, same results */
 } jfc_params;
 
 /* Capacity model (replaces computeCapacity / kmeans / computeExcessFlowLazy,

@@ -111,6 +111,8 @@ static void tileset_carve(TileSet& ts, char* blk, size_t* total) {
   const size_t o_gact = take(sizeof(int) * ng);
   const size_t o_sum = take(sizeof(long long) * 2 * ng);
   const size_t o_ctr = take(sizeof(DevCounters));
+  const size_t o_ring = take(sizeof(unsigned long long) * nt * 2);   // work items: halves of split tiles
+  const size_t o_lock = take(sizeof(int) * nt * 2);
   *total = off;
   if (!blk) return;
   ts.d_desc = (GridDev*)(blk + o_desc);
@@ -126,6 +128,8 @@ static void tileset_carve(TileSet& ts, char* blk, size_t* total) {
   ts.d_grid_active = (int*)(blk + o_gact);
   ts.d_grid_sum = (long long*)(blk + o_sum);
   ts.d_ctr = (DevCounters*)(blk + o_ctr);
+  ts.d_pr_ring = (unsigned long long*)(blk + o_ring);
+  ts.d_pr_lock = (int*)(blk + o_lock);
 }
 
 int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const std::vector<GridDev>& grids_in,
@@ -236,9 +240,10 @@ static size_t pin_need(const TileSet& ts) {
   return sizeof(DevCounters) + sizeof(long long) * 2 * (size_t)ts.ngrids + 64;
 }
 
-// pinned slot holding the sweep pairs of the next push-relabel phase and the
-// distance cap of the relabel after it (after the read-back area); copied to
-// the control block (pr_sweeps, h_cap) by the cycle itself
+// pinned slot holding the sweep pairs of the next push-relabel phase, the
+// distance cap of the relabel after it and whether that relabel may skip
+// frozen tiles (after the read-back area); copied to the control block
+// (pr_sweeps, h_cap, skip_frozen) by the cycle itself
 static int* pin_sweeps(jfc_ctx* ctx, const TileSet& ts) {
   return (int*)((char*)ctx->h_pin + (pin_need(ts) + 255) / 256 * 256);
 }
@@ -305,7 +310,7 @@ int engine_bfs(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, bool cut, int& pa
 namespace {
 struct CycleGraphs {
   struct Entry {
-    int local_iters, max_passes;
+    int local_iters, max_passes, sched;
     void* pin;
     cudaGraphExec_t exec;
   };
@@ -322,24 +327,25 @@ void tileset_drop_graphs(TileSet& ts) {
   ts.gcache = nullptr;
 }
 
-static cudaError_t enqueue_cycle(TileSet& ts, const int* pin_sw, int local_iters, int max_passes, cudaStream_t s,
-                                 void* pin) {
+static cudaError_t enqueue_cycle(TileSet& ts, const int* pin_sw, int local_iters, int max_passes, int sched,
+                                 cudaStream_t s, void* pin) {
   cudaError_t e = cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s);
-  static_assert(offsetof(DevCounters, h_cap) == offsetof(DevCounters, pr_sweeps) + sizeof(int),
-                "pr_sweeps and h_cap are copied together");
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&ts.d_ctr->pr_sweeps, pin_sw, 2 * sizeof(int), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = launch_pr_phase(ts, 0, local_iters, s);
+  static_assert(offsetof(DevCounters, h_cap) == offsetof(DevCounters, pr_sweeps) + sizeof(int) &&
+                    offsetof(DevCounters, skip_frozen) == offsetof(DevCounters, pr_sweeps) + 2 * sizeof(int),
+                "pr_sweeps, h_cap and skip_frozen are copied together");
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&ts.d_ctr->pr_sweeps, pin_sw, 3 * sizeof(int), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = launch_pr_phase(ts, 0, local_iters, s, sched);
   if (e == cudaSuccess) e = enqueue_bfs(ts, false, max_passes, s, pin);
   return e;
 }
 
-static cudaGraphExec_t cycle_graph(TileSet& ts, const int* pin_sw, int local_iters, int max_passes, cudaStream_t s,
-                                   void* pin) {
+static cudaGraphExec_t cycle_graph(TileSet& ts, const int* pin_sw, int local_iters, int max_passes, int sched,
+                                   cudaStream_t s, void* pin) {
   if (!ts.gcache) ts.gcache = new CycleGraphs();
   CycleGraphs* c = (CycleGraphs*)ts.gcache;
   if (c->broken) return nullptr;
   for (auto& e : c->v)
-    if (e.local_iters == local_iters && e.max_passes == max_passes && e.pin == pin)
+    if (e.local_iters == local_iters && e.max_passes == max_passes && e.sched == sched && e.pin == pin)
       return e.exec;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
@@ -352,7 +358,7 @@ static cudaGraphExec_t cycle_graph(TileSet& ts, const int* pin_sw, int local_ite
     return nullptr;
   }
   g_capturing = true;
-  const cudaError_t e1 = enqueue_cycle(ts, pin_sw, local_iters, max_passes, s, pin);
+  const cudaError_t e1 = enqueue_cycle(ts, pin_sw, local_iters, max_passes, sched, s, pin);
   g_capturing = false;
   cudaGraph_t g = nullptr;
   const cudaError_t e2 = cudaStreamEndCapture(s, &g);
@@ -366,7 +372,7 @@ static cudaGraphExec_t cycle_graph(TileSet& ts, const int* pin_sw, int local_ite
     c->broken = true;
     return nullptr;
   }
-  c->v.push_back({local_iters, max_passes, pin, x});
+  c->v.push_back({local_iters, max_passes, sched, pin, x});
   return x;
 }
 
@@ -380,14 +386,16 @@ static int run_cycle(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, int interva
   int* pin_sw = pin_sweeps(ctx, ts);
   pin_sw[0] = interval;   // the previous cycle's copies finished at its sync
   pin_sw[1] = h_cap;
-  cudaGraphExec_t x = p.use_graph ? cycle_graph(ts, pin_sw, p.local_iters, p.max_bfs_passes, s, ctx->h_pin)
+  pin_sw[2] = 1;          // within a solve, after its first relabel: frozen tiles are skipped
+  const int sched = pr_sched_for(p);
+  cudaGraphExec_t x = p.use_graph ? cycle_graph(ts, pin_sw, p.local_iters, p.max_bfs_passes, sched, s, ctx->h_pin)
                                   : nullptr;
   if (x) {
     JFC_CUDA(cudaGraphLaunch(x, s));
     jfc_note_launch(2);
     if (used_graph) *used_graph = true;
   } else {
-    JFC_CUDA(enqueue_cycle(ts, pin_sw, p.local_iters, p.max_bfs_passes, s, ctx->h_pin));
+    JFC_CUDA(enqueue_cycle(ts, pin_sw, p.local_iters, p.max_bfs_passes, sched, s, ctx->h_pin));
   }
   JFC_CUDA(cudaStreamSynchronize(s));
   return finish_bfs(ts, false, ctx->h_pin, passes, &active, nullptr, sweeps_done);

@@ -24,6 +24,14 @@
 #define JFC_PAD_Z3 4        // 3D z padding (tile depths 1, 2, 4)
 #define JFC_MAX_K 32        // k-means clusters per class
 #define JFC_TQ 65536        // t-link probability quantisation
+// Tile activity byte: the dense relabel pass gave the tile no finite height
+// (no deficit in it, none across a residual arc from its halo) and no later
+// relabel visit lowered one.  Push-relabel never enters such a tile (its
+// nodes are inactive and nothing pushes into an unreachable node) and
+// deficits never appear, so its excess, arcs, heights and arc bytes stay as
+// they are and the dense pass of a later relabel in the same solve would give
+// the same result: that pass skips it.
+#define JFC_ACT_FROZEN 4u
 
 // Device-side descriptor of one grid instance.
 struct GridDev {
@@ -52,8 +60,9 @@ struct DevCounters {
   int bfs_status;            // 1 converged, 2 pass budget exhausted
   int sweeps_done;           // sweeps run by the last push-relabel phase
   int pr_sweeps;             // sweep pairs of the next phase when launched with sweeps <= 0
-  int h_cap;                 // global relabels: distances >= h_cap count as unreachable (0: no cap);
-                             // adjacent to pr_sweeps: a relabel cycle copies both at once
+  int h_cap;                 // global relabels: distances >= h_cap count as unreachable (0: no cap)
+  int skip_frozen;           // global relabels: the dense pass skips frozen tiles (JFC_ACT_FROZEN);
+                             // pr_sweeps, h_cap, skip_frozen: a relabel cycle copies them at once
   int fast_moved;            // a Fast-Cut push moved flow (comparison mode)
   unsigned long long visits; // push-relabel tile visits
   unsigned long long bfs_visits;
@@ -64,6 +73,9 @@ struct DevCounters {
   unsigned long long t_gr_start;      // device clock at the start of the last relabel
   unsigned long long prof[8];         // SM-cycle split of push-relabel visits (JFC_PHASE_CLOCK builds)
   unsigned long long spin_limit;  // polls before a device-side wait gives up (0: 2^26)
+  unsigned pr_head;          // push-relabel worklist: tickets taken
+  unsigned pr_tail;          // push-relabel worklist: ring positions reserved
+  int pr_out;                // push-relabel worklist: items queued and not yet fully visited
   unsigned wl_head;          // 2D relabel worklist: tickets taken
   unsigned wl_tail;          // 2D relabel worklist: ring positions reserved
   int wl_out;                // 2D relabel worklist: items queued and not yet fully visited
@@ -85,8 +97,11 @@ struct TileSet {
   int* d_q_pr[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [parity][buffer]
   int* d_flag_bfs[2] = {nullptr, nullptr};  // [buffer][ntiles] tile waits in a BFS frontier
   int* d_q_bfs[2] = {nullptr, nullptr};     // [buffer] BFS frontiers
-  uint8_t* d_act = nullptr;          // [ntiles] tile held an active node at its last relabel visit
+  uint8_t* d_act = nullptr;          // [ntiles] bits 0-1: tile (half) held an active node at its last
+                                     // relabel visit; JFC_ACT_FROZEN: see below
   int* d_grid_active = nullptr;      // [ngrids] active tiles after global relabel
+  unsigned long long* d_pr_ring = nullptr;  // [work items] push-relabel worklist ring (null: sweeps only)
+  int* d_pr_lock = nullptr;          // [work items] a visit of the item is in progress
   long long* d_grid_sum = nullptr;   // [ngrids*2] sum min(e,0), source-side count
   DevCounters* d_ctr = nullptr;
   void* d_block = nullptr;           // single allocation backing the above
@@ -120,7 +135,9 @@ void jfc_note_launch(int n = 1);
 // in one persistent launch, draining the device work queues; sweeps <= 0
 // reads the count from the control block (pr_sweeps), so one captured graph
 // serves every interval
-cudaError_t launch_pr_phase(const TileSet& ts, int sweeps, int local_iters, cudaStream_t s);
+// sched 2: the asynchronous worklist (needs ts.d_pr_ring) instead of the
+// parity sweeps
+cudaError_t launch_pr_phase(const TileSet& ts, int sweeps, int local_iters, cudaStream_t s, int sched = 1);
 // Local pre-push inside every tile before the first relabel of a solve.
 cudaError_t launch_prepush(const TileSet& ts, cudaStream_t s);
 // (kernels_bfs.cu) one BFS to its fixpoint in one persistent launch:

@@ -534,8 +534,8 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
     if (W.ring) ring_append(want, nb, Q.flags, W);
     else jfc::warp_append(want, nb, Q.flags, Q.q, Q.qn);
     if (t == 0) {
-      const int old = (fresh ? __ldcg(ts.d_act + tid) : ts.d_act[tid]) != 0 ? 1 : 0;
-      ts.d_act[tid] = (uint8_t)((act_lo ? 1 : 0) | (act_hi ? 2 : 0));
+      const int old = ((fresh ? __ldcg(ts.d_act + tid) : ts.d_act[tid]) & 3u) != 0 ? 1 : 0;
+      ts.d_act[tid] = (uint8_t)((act_lo ? 1 : 0) | (act_hi ? 2 : 0));   // a visited tile is not frozen
       if (ti.x != cur_grid) {
         if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
         delta = 0;
@@ -559,6 +559,10 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
   using D = Dirs<DIMS>;
   constexpr int R = TY * TZ;
   const int lane = threadIdx.x & 31;
+  // a frozen tile would get the same (all unreachable) result again
+#ifndef JFC_NO_FROZEN_SKIP
+  if (jfc::vload(&ts.d_ctr->skip_frozen) && (ts.d_act[tid] & JFC_ACT_FROZEN)) return;
+#endif
   const int4 ti = ts.d_info[tid];
   const GridDev& g = ts.d_desc[ti.x];
   const Addr a = make_addr<DIMS, TY, TZ>(g, ti, lane);
@@ -661,9 +665,10 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
       if ((N[i] >> lane) & 1u) h[i] = d + 1;
     }
   }
-  unsigned rows_fin = 0, c0 = 0, c31 = 0, act = 0, act_hi = 0;
+  unsigned rows_fin = 0, c0 = 0, c31 = 0, act = 0, act_hi = 0, any_finite = 0;
 #pragma unroll
   for (int i = 0; i < R; ++i) {
+    any_finite |= V[i];
     g.h[roff<TY>(a, i)] = h[i];
     const unsigned fin = V[i] & ~DEF[i];   // finite and above 0: news for the neighbours
     if (fin) rows_fin |= 1u << i;
@@ -675,7 +680,7 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
   }
   if (lane == 0) {
     const int old = 0;
-    ts.d_act[tid] = (uint8_t)((act ? 1 : 0) | (act_hi ? 2 : 0));
+    ts.d_act[tid] = (uint8_t)((act ? 1 : 0) | (act_hi ? 2 : 0) | (any_finite ? 0u : JFC_ACT_FROZEN));
     act |= act_hi;
     if (ti.x != cur_grid) {
       if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
@@ -823,8 +828,8 @@ __device__ __forceinline__ void relabel_frontier_warp(const TileSet& ts, int tid
   for (int i = 0; i < R; ++i) act |= ((posm >> i) & 1u) && hv[i] < JFC_INF;
   act = __any_sync(FULL, act);
   if (lane == 0) {
-    const int old = ts.d_act[tid] != 0 ? 1 : 0;
-    ts.d_act[tid] = act ? 1 : 0;
+    const int old = (ts.d_act[tid] & 3u) != 0 ? 1 : 0;
+    ts.d_act[tid] = act ? 1 : 0;   // a visited tile is not frozen
     if (ti.x != cur_grid) {
       if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
       delta = 0;
@@ -851,7 +856,7 @@ __device__ __forceinline__ void refill_pr_queues(const TileSet& ts, DevCounters*
     const long long t = b + lane;
     bool w[2][2] = {{false, false}, {false, false}};   // [half][parity queue]
     if (t < ts.ntiles) {
-      const unsigned bits = ts.d_act[t];
+      const unsigned bits = ts.d_act[t] & 3u;
       int par = 0;
       if (bits) { const int4 ti = ts.d_info[t]; par = (ti.y + (ts.pr_split ? 2 * ti.z : ti.z) + ti.w) & 1; }
       if (ts.pr_split) {
@@ -902,7 +907,10 @@ __global__ void __launch_bounds__(256, (DIMS == 3 && TY * TZ > 8) ? 1 : (DIMS ==
 // Warp form of the frontier passes: one warp per queued tile (3D: many
 // tiles per pass, so the visit throughput counts).
 template <int DIMS, int TY, int TZ>
-__global__ void __launch_bounds__(256) k_relabel_warp(TileSet ts, int max_passes) {
+#ifndef JFC_RELABEL_WARP_MINB
+#define JFC_RELABEL_WARP_MINB 1
+#endif
+__global__ void __launch_bounds__(256, JFC_RELABEL_WARP_MINB) k_relabel_warp(TileSet ts, int max_passes) {
   DevCounters* ctr = ts.d_ctr;
   const int lane = threadIdx.x & 31;
   unsigned long long visits = 0;

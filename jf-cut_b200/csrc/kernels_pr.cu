@@ -52,7 +52,10 @@ struct PrSmem {
   int out[T::NHALO];      // flow pushed into each halo cell during the visit
   uint8_t arc[T::NT];     // residual-arc bits for the local relabel
   int tile;
+  int gen;                // worklist: generation of the item being visited
   int face[6];            // any flow left through face: x-, x+, y-, y+, z-, z+
+  int q_nb[6];            // after a visit: the work item behind each face that received flow, or -1
+  int active;             // after a visit: the item still holds an active node
 };
 
 template <int DIMS, int TY, int TZ>
@@ -63,9 +66,32 @@ __device__ __forceinline__ void halo_cell(int c, int& x, int& y, int& z, int& fa
 // SPLIT: the work item `tid` is half `tid & 1` (rows 0-7 / 8-15) of the 2D
 // 32x16 tile `tid >> 1`, visited as a 32x8 tile; the halves keep their own
 // checkerboard parity, so the two halves of a tile never run at once.
+// The work items behind the faces of item `tid` (x-, x+, y-, y+, z-, z+),
+// -1 where the face is the grid's border.
+template <int DIMS, int TY, int TZ, bool SPLIT>
+__device__ __forceinline__ int face_item(const TileSet& ts, int tid, int f) {
+  const int tile = SPLIT ? tid >> 1 : tid, half = SPLIT ? tid & 1 : 0;
+  const int4 ti = ts.d_info[tile];
+  const GridDev& g = ts.d_desc[ti.x];
+  const int txs = g.tiles_x, tys = g.tiles_y, tzs = g.tiles_z;
+  switch (f) {
+    case 0: return ti.y > 0 ? (SPLIT ? tid - 2 : tid - 1) : -1;
+    case 1: return ti.y < txs - 1 ? (SPLIT ? tid + 2 : tid + 1) : -1;
+    case 2: return SPLIT ? (half ? tid - 1 : (ti.z > 0 ? 2 * (tile - txs) + 1 : -1)) : (ti.z > 0 ? tid - txs : -1);
+    case 3: return SPLIT ? (half ? (ti.z < tys - 1 ? 2 * (tile + txs) : -1) : tid + 1)
+                         : (ti.z < tys - 1 ? tid + txs : -1);
+    case 4: return DIMS == 3 && ti.w > 0 ? tid - txs * tys : -1;
+    case 5: return DIMS == 3 && ti.w < tzs - 1 ? tid + txs * tys : -1;
+    default: return -1;
+  }
+}
+
+// One visit of work item `tid`; on return s.active tells whether the item still
+// holds an active node and s.q_nb[f] the item behind each face f that
+// received flow (-1: none).  The caller queues them.
 template <int DIMS, int TY, int TZ, bool SPLIT>
 __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_iters, bool local_relabel,
-                                        PrSmem<DIMS, TY, TZ>& s, int* self_q, int* self_n, int* nbr_q, int* nbr_n) {
+                                        PrSmem<DIMS, TY, TZ>& s) {
   using T = Tile<DIMS, TY, TZ>;
   const int t = threadIdx.x;
   const int x = t & 31, row = t >> 5, y = row % TY, z = row / TY;
@@ -120,17 +146,19 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
   }
   __syncthreads();
   JFC_PCLK(ts.d_ctr, 0);
+  // the node's own height lives in a register for the rounds (only its owner
+  // writes it); the shared copy is what the neighbours read
+  int hown = h0;
   if (JFC_LOCAL_RELABEL_ITERS > 0 && local_relabel) {
     // a partial relaxation overestimates distances, so the local labelling
     // is only applied when the in-tile fixpoint was reached
     const bool exact = jfc::relax_cta<DIMS, TY, TZ>(s.h, s.arc, JFC_LOCAL_RELABEL_ITERS);
-    s.h[hi] = exact ? max(s.h[hi], h0) : h0;
+    hown = exact ? max(s.h[hi], h0) : h0;
 #ifdef JFC_PHASE_CLOCK
     if (threadIdx.x == 0 && exact) atomicAdd(&ts.d_ctr->prof[5], 1ull);
 #endif
-  } else {
-    s.h[hi] = h0;
   }
+  s.h[hi] = hown;
   __syncthreads();
   JFC_PCLK(ts.d_ctr, 1);
 
@@ -141,62 +169,63 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
   const int hc_ym = z * 32 + x, hc_yp = TZ * 32 + z * 32 + x;
   const int hc_zm = T::NHY + T::NHX + y * 32 + x, hc_zp = T::NHY + T::NHX + TY * 32 + y * 32 + x;
 
+  // push order: +x, +y, -y, (+z, -z,) -x; q is a constant after unrolling
+  constexpr int NP = DIMS == 3 ? 6 : 4;
+  auto slot = [](int q) { return q == 0 ? T::XP : q == 1 ? T::YP : q == 2 ? T::YM
+                                        : q == NP - 1 ? T::XM : q == 3 ? T::ZP : T::ZM; };
+  auto hoff = [](int q) { return q == 0 ? 1 : q == 1 ? T::HX : q == 2 ? -T::HX
+                                       : q == NP - 1 ? -1 : q == 3 ? T::HX * T::HY : -T::HX * T::HY; };
+  auto toff = [](int q) { return q == 0 ? 1 : q == 1 ? 32 : q == 2 ? -32
+                                       : q == NP - 1 ? -1 : q == 3 ? 32 * TY : -32 * TY; };
   int it = 0;
   for (; it < local_iters; ++it) {
     bool did = false;
+    // the node's excess and residual arcs, read once per round: nothing
+    // changes them between the relabel step and the push step, and the
+    // credits neighbours add during the push step only raise them, so these
+    // values bound what the node may push from below
+    const int e = s.e[t];
+    const bool act = e > 0 && hown < JFC_INF;
+    int rk[NP];
     // relabel every active node without an admissible arc, in place
     // (graphcut_push_relabel.cl:80-99 relabels two colours in turn).  A node
     // reading a neighbour that relabels in the same step sees its old or new
     // height; heights only grow, so either value keeps the labelling valid.
-    {
-      const int h = s.h[hi];
-      if (s.e[t] > 0 && h < JFC_INF) {
-        const int hxp = s.h[hi + 1], hxm = s.h[hi - 1];
-        const int hyp = s.h[hi + T::HX], hym = s.h[hi - T::HX];
-        const int rxp = s.r[T::XP][t], ryp = s.r[T::YP][t], rym = s.r[T::YM][t], rxm = s.r[T::XM][t];
-        const int hm = h - 1;
-        bool adm = (rxp > 0 && hxp == hm) | (ryp > 0 && hyp == hm) | (rym > 0 && hym == hm) |
-                   (rxm > 0 && hxm == hm);
-        int m = min(min(rxp > 0 ? hxp : JFC_INF, ryp > 0 ? hyp : JFC_INF),
-                    min(rym > 0 ? hym : JFC_INF, rxm > 0 ? hxm : JFC_INF));
-        if constexpr (DIMS == 3) {
-          const int hzp = s.h[hi + T::HX * T::HY], hzm = s.h[hi - T::HX * T::HY];
-          const int rzp = s.r[T::ZP][t], rzm = s.r[T::ZM][t];
-          adm |= (rzp > 0 && hzp == hm) | (rzm > 0 && hzm == hm);
-          m = min(m, min(rzp > 0 ? hzp : JFC_INF, rzm > 0 ? hzm : JFC_INF));
-        }
-        if (!adm) {
-          s.h[hi] = max(h, min(m + 1, JFC_INF));
-          did = true;
-        }
+    if (act) {
+      int hn[NP];
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        rk[q] = s.r[slot(q)][t];
+        hn[q] = s.h[hi + hoff(q)];
       }
-      __syncthreads();
+      const int hm = hown - 1;
+      bool adm = false;
+      int m = JFC_INF;
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        adm |= rk[q] > 0 && hn[q] == hm;
+        m = min(m, rk[q] > 0 ? hn[q] : JFC_INF);
+      }
+      if (!adm) {
+        hown = max(hown, min(m + 1, JFC_INF));
+        s.h[hi] = hown;
+        did = true;
+      }
     }
+    __syncthreads();
     // push: every node with excess, along admissible arcs in reference order.
     // All operands are loaded first and the pushes are computed in registers,
     // then issued as independent shared-memory updates: a push u->v needs
     // h(u) = h(v) + 1, so in one step nothing else writes u's own arcs or the
     // reverse arc v->u that u credits (the credits are reductions, no load).
     {
-      const int h = s.h[hi];
-      const int e = s.e[t];
-      if (e > 0 && h < JFC_INF) {
-        const int hm = h - 1;
-        constexpr int NP = DIMS == 3 ? 6 : 4;
-        // push order: +x, +y, -y, (+z, -z,) -x; q is a constant after unrolling
-        auto slot = [](int q) { return q == 0 ? T::XP : q == 1 ? T::YP : q == 2 ? T::YM
-                                              : q == NP - 1 ? T::XM : q == 3 ? T::ZP : T::ZM; };
-        auto hoff = [](int q) { return q == 0 ? 1 : q == 1 ? T::HX : q == 2 ? -T::HX
-                                             : q == NP - 1 ? -1 : q == 3 ? T::HX * T::HY : -T::HX * T::HY; };
-        auto toff = [](int q) { return q == 0 ? 1 : q == 1 ? 32 : q == 2 ? -32
-                                             : q == NP - 1 ? -1 : q == 3 ? 32 * TY : -32 * TY; };
+      if (act && hown < JFC_INF) {
+        const int hm = hown - 1;
         const bool inside[6] = {in_xp, in_yp, in_ym, DIMS == 3 ? in_zp : in_xm, in_zm, in_xm};
         const int hcell[6] = {hc_xp, hc_yp, hc_ym, DIMS == 3 ? hc_zp : hc_xm, hc_zm, hc_xm};
-        int hn[NP], rk[NP], d[NP];
+        int hn[NP], d[NP];
 #pragma unroll
         for (int q = 0; q < NP; ++q) hn[q] = s.h[hi + hoff(q)];
-#pragma unroll
-        for (int q = 0; q < NP; ++q) rk[q] = s.r[slot(q)][t];
         int ex = e;
 #pragma unroll
         for (int q = 0; q < NP; ++q) {
@@ -227,7 +256,7 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
   JFC_PCLK(ts.d_ctr, 2);
 
   // ---- write back the words that changed
-  const int e1 = s.e[t], h1 = s.h[hi];
+  const int e1 = s.e[t], h1 = hown;
   if (e1 != e0) g.e[n] = e1;
   if (h1 != h0) g.h[n] = h1;
 #pragma unroll
@@ -252,24 +281,10 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
     }
   }
   const bool active = __syncthreads_or((e1 > 0) & (h1 < JFC_INF));
-  // ---- queue: myself for my parity's next sweep, neighbours for the other parity
-  if (t < 32) {
-    const int txs = g.tiles_x, tys = g.tiles_y;
-    bool want = false;
-    int nb = tid;
-    switch (t) {
-      case 0: want = s.face[0]; nb = SPLIT ? tid - 2 : tid - 1; break;
-      case 1: want = s.face[1]; nb = SPLIT ? tid + 2 : tid + 1; break;
-      case 2: want = s.face[2]; nb = SPLIT ? (half ? tid - 1 : 2 * (tile - txs) + 1) : tid - txs; break;
-      case 3: want = s.face[3]; nb = SPLIT ? (half ? 2 * (tile + txs) : tid + 1) : tid + txs; break;
-      case 4: want = DIMS == 3 && s.face[4]; nb = tid - txs * tys; break;
-      case 5: want = DIMS == 3 && s.face[5]; nb = tid + txs * tys; break;
-      default: break;
-    }
-    jfc::warp_append(want, nb, ts.d_flag_pr, nbr_q, nbr_n);
-    if (active && t == 0) ts.d_flag_pr[tid] = 1;
-    jfc::warp_append(active && t == 0, tid, nullptr, self_q, self_n);
-  }
+  // flow crossed face f only toward an item inside the grid (arcs leaving
+  // the grid are zero)
+  if (t < 6) s.q_nb[t] = s.face[t] ? face_item<DIMS, TY, TZ, SPLIT>(ts, tid, t) : -1;
+  if (t == 0) s.active = active ? 1 : 0;
   __syncthreads();
   JFC_PCLK(ts.d_ctr, 3);
   return rounds;
@@ -307,9 +322,18 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
       // first sweep of a phase: nothing moved since the exact global relabel
       // (the halo tiles have the other parity), so the local relabel would
       // reproduce the heights it finds
-      rounds += pr_visit<DIMS, TY, TZ, SPLIT>(ts, tid, local_iters, s > 0, sm, ts.d_q_pr[p][b ^ 1],
-                                              &ctr->qn_pr[p][b ^ 1], ts.d_q_pr[p ^ 1][bo], &ctr->qn_pr[p ^ 1][bo]);
+      rounds += pr_visit<DIMS, TY, TZ, SPLIT>(ts, tid, local_iters, s > 0, sm);
       ++visits;
+      // queue: myself for my parity's next sweep, neighbours for the other parity
+      if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        const int nb = lane < 6 ? sm.q_nb[lane] : -1;
+        jfc::warp_append(nb >= 0, nb, ts.d_flag_pr, ts.d_q_pr[p ^ 1][bo], &ctr->qn_pr[p ^ 1][bo]);
+        const bool active = sm.active != 0;
+        if (active && lane == 0) ts.d_flag_pr[tid] = 1;
+        jfc::warp_append(active && lane == 0, tid, nullptr, ts.d_q_pr[p][b ^ 1], &ctr->qn_pr[p][b ^ 1]);
+      }
+      __syncthreads();
     }
     JFC_PCLK_DECL
     const bool ok = jfc::grid_sync(ctr, [&]() {
@@ -330,16 +354,200 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Asynchronous push-relabel phase: a worklist instead of parity sweeps.
+//
+// The sweeps keep adjacent work items apart by running one checkerboard
+// colour at a time, with a grid barrier between colours; in the tail of a
+// solve a sweep holds a few items and every CTA waits at the barrier for the
+// slowest visit.  Here the items live in a ring (one entry per queued item:
+// the queued flags dedupe), any free CTA takes the next entry, and adjacency
+// is kept apart by per-item locks instead: a visit takes its item's lock,
+// then (after a sequentially consistent fence) checks that no item behind
+// its faces holds one; of two adjacent items that try at once at least one
+// sees the other and backs off (the entry goes back to the ring).  So a visit
+// sees exactly what it would see in a sweep: its item and halo untouched by
+// any other visit while it runs.  An entry carries a generation that plays
+// the role of the sweep index: a visit of generation k queues the items it
+// fed for k + 1 (the other colour's next sweep) and itself for k + 2 (its own
+// colour's next sweep), and a phase of `npairs` sweep pairs visits
+// generations 0 .. 2 * npairs - 1 (the sweeps' budget); items past it stay
+// active for the next global relabel.  The phase ends when
+// no queued item is left (every wait is bounded, see jfc::spin_cap).
+constexpr unsigned long long kRingEmpty = ~0ull;
+
+__device__ __forceinline__ unsigned long long ring_entry(int item, int gen) {
+  return ((unsigned long long)(unsigned)gen << 32) | (unsigned)item;
+}
+
+// Put one entry into the ring (a position reserved at the tail; the slot is
+// free, or freed by its reader within a few polls).  Returns false after an
+// error.
+__device__ __forceinline__ bool pr_ring_put(unsigned long long* ring, unsigned cap, unsigned* tail, int* err,
+                                            unsigned long long max_spins, unsigned long long v) {
+  const unsigned pos = atomicAdd(tail, 1u);
+  unsigned long long* slot = ring + pos % cap;
+  unsigned long long spins = 0;
+  while (atomicCAS(slot, kRingEmpty, v) != kRingEmpty) {
+    if (++spins > max_spins || jfc::vload(err)) { atomicExch(err, 1); return false; }
+    __nanosleep(32);
+  }
+  return true;
+}
+
+template <int DIMS, int TY, int TZ, bool SPLIT>
+__global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
+    k_pr_async(TileSet ts, int sweeps, int local_iters) {
+  __shared__ PrSmem<DIMS, TY, TZ> sm;
+  DevCounters* ctr = ts.d_ctr;
+  const unsigned long long t0 = jfc::global_ns();
+  const int npairs = sweeps > 0 ? sweeps : jfc::vload(&ctr->pr_sweeps);
+  const int gens = 2 * npairs;
+  const unsigned cap = (unsigned)(SPLIT ? 2 * ts.ntiles : ts.ntiles);
+  unsigned long long* ring = ts.d_pr_ring;
+  int* lock = ts.d_pr_lock;
+  // ---- the ring starts with the items the global relabel queued (both
+  //      parity queues, colour 0 first: the first wave of takers is
+  //      conflict-free), generation 0; locks clear
+  const int b0 = jfc::vload(&ctr->cur_pr[0]), b1 = jfc::vload(&ctr->cur_pr[1]);
+  const int n0 = jfc::vload(&ctr->qn_pr[0][b0]), n1 = jfc::vload(&ctr->qn_pr[1][b1]);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cap; i += (long long)gridDim.x * blockDim.x) {
+    unsigned long long v = kRingEmpty;
+    if (i < n0) v = ring_entry(ts.d_q_pr[0][b0][i], 0);
+    else if (i < n0 + n1) v = ring_entry(ts.d_q_pr[1][b1][i - n0], 0);
+    ring[i] = v;
+    lock[i] = 0;
+  }
+  const bool ok = jfc::grid_sync(ctr, [&]() {
+    ctr->pr_head = 0;
+    ctr->pr_tail = (unsigned)(n0 + n1);
+    ctr->pr_out = n0 + n1;
+    ctr->sweeps_done = 0;
+  });
+  const unsigned long long max_spins = jfc::spin_cap(ctr);
+  unsigned long long visits = 0, rounds = 0;
+  int maxgen = -1;
+  while (ok) {
+    if (threadIdx.x == 0) {
+      int item = -1, gen = 0;
+      const unsigned k = atomicAdd(&ctr->pr_head, 1u);
+      unsigned long long* slot = ring + k % cap;
+      // bounded: the entry arrives, or no item is left, or an error; the
+      // count restarts whenever the worklist moves
+      unsigned long long spins = 0, v = kRingEmpty;
+      unsigned seen_tail = (unsigned)jfc::vload((const int*)&ctr->pr_tail);
+      int seen_out = jfc::vload(&ctr->pr_out);
+      for (;;) {
+        if (*(volatile unsigned long long*)slot != kRingEmpty) {
+          v = atomicExch(slot, kRingEmpty);
+          if (v != kRingEmpty) break;
+        }
+        const int out = jfc::vload(&ctr->pr_out);
+        if (out == 0 || jfc::vload(&ctr->error)) break;
+        const unsigned tl = (unsigned)jfc::vload((const int*)&ctr->pr_tail);
+        if (out != seen_out || tl != seen_tail) {
+          seen_out = out;
+          seen_tail = tl;
+          spins = 0;
+        } else if (++spins > max_spins) {
+          atomicExch(&ctr->error, 1);
+          break;
+        }
+        __nanosleep(32);
+      }
+      if (v != kRingEmpty) {
+        item = (int)(unsigned)(v & 0xffffffffu);
+        gen = (int)(v >> 32);
+        // neighbour exclusion (see above)
+        bool conflict = atomicCAS(lock + item, 0, 1) != 0;
+        if (!conflict) {
+          asm volatile("fence.sc.gpu;" ::: "memory");
+#pragma unroll
+          for (int f = 0; f < (DIMS == 3 ? 6 : 4); ++f) {
+            const int nb = face_item<DIMS, TY, TZ, SPLIT>(ts, item, f);
+            if (nb >= 0 && jfc::vload(lock + nb) != 0) conflict = true;
+          }
+          if (conflict) atomicExch(lock + item, 0);
+        }
+        if (conflict) {
+          // back to the ring, same generation, still flagged as queued (it
+          // stays outstanding); -2: take the next entry
+          if (!pr_ring_put(ring, cap, &ctr->pr_tail, &ctr->error, max_spins, v)) item = -1;
+          else item = -2;
+        } else {
+          ts.d_flag_pr[item] = 0;   // dequeued: a neighbour may queue it again once we unlock
+          __threadfence();
+        }
+      }
+      sm.tile = item;
+      sm.gen = gen;
+    }
+    __syncthreads();
+    const int item = sm.tile, gen = sm.gen;
+    if (item == -1) break;
+    if (item == -2) {
+      __syncthreads();   // sm.tile is rewritten only after every thread read it
+      continue;
+    }
+    // generation 0: nothing around the item moved since the exact global
+    // relabel unless a neighbour was visited first; the local relabel is an
+    // improvement only, so skipping it is safe either way
+    rounds += pr_visit<DIMS, TY, TZ, SPLIT>(ts, item, local_iters, gen > 0, sm);
+    ++visits;
+    maxgen = max(maxgen, gen);
+    // release the item (its writes visible first), then queue what it fed
+    // and itself for generation gen + 1, then count it done
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicExch(lock + item, 0);
+    }
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      int nb = -1, ng = gen + 1;
+      if (lane < 6) nb = sm.q_nb[lane];
+      else if (lane == 6 && sm.active) { nb = item; ng = gen + 2; }
+      bool won = false;
+      if (ng < gens && nb >= 0) won = atomicExch(ts.d_flag_pr + nb, 1) == 0;
+      const unsigned m = __ballot_sync(jfc::FULL, won);
+      if (m && lane == 0) atomicAdd(&ctr->pr_out, __popc(m));   // counted before they can finish
+      // (a failed put raises the error flag; the next dequeue sees it and
+      // every thread of the CTA leaves the loop together)
+      if (won) pr_ring_put(ring, cap, &ctr->pr_tail, &ctr->error, max_spins, ring_entry(nb, ng));
+      __syncwarp();
+      if (lane == 0) atomicSub(&ctr->pr_out, 1);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (visits) atomicAdd(&ctr->visits, visits);
+    if (rounds) atomicAdd(&ctr->rounds, rounds);
+    // "sweeps" of the phase: generations reached (the engine's schedule reads it)
+    atomicMax(&ctr->sweeps_done, maxgen + 1);
+  }
+  // the phase clock: the last CTA to leave adds the elapsed time
+  __shared__ bool s_last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&ctr->bar_count, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && s_last) {
+    ctr->bar_count = 0;
+    ctr->ns_pr += jfc::global_ns() - t0;
+  }
+}
+
 template <int DIMS, int TY, int TZ, bool SPLIT = false>
-cudaError_t launch_t(const TileSet& ts, int sweeps, int local_iters, cudaStream_t st) {
+cudaError_t launch_t(const TileSet& ts, int sweeps, int local_iters, cudaStream_t st, int sched) {
   constexpr int NT = Tile<DIMS, TY, TZ>::NT;
-  static int cache[64] = {0};
-  const int blocks = persistent_blocks_cached(cache, (const void*)k_pr_phase<DIMS, TY, TZ, SPLIT>, NT);
+  const bool async = sched == 2 && ts.d_pr_ring != nullptr;
+  const void* fn = async ? (const void*)k_pr_async<DIMS, TY, TZ, SPLIT> : (const void*)k_pr_phase<DIMS, TY, TZ, SPLIT>;
+  static int cache_sweeps[64] = {0}, cache_async[64] = {0};
+  const int blocks = persistent_blocks_cached(async ? cache_async : cache_sweeps, fn, NT);
   TileSet arg = ts;
   void* params[] = {(void*)&arg, (void*)&sweeps, (void*)&local_iters};
   jfc_note_launch();
-  return cudaLaunchCooperativeKernel((const void*)k_pr_phase<DIMS, TY, TZ, SPLIT>, dim3(blocks), dim3(NT), params, 0,
-                                     st);
+  return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(NT), params, 0, st);
 }
 
 // Local pre-push before the first relabel of a solve, one CTA per tile, the
@@ -428,19 +636,19 @@ cudaError_t launch_prepush(const TileSet& ts, cudaStream_t s) {
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_pr_phase(const TileSet& ts, int sweeps, int local_iters, cudaStream_t s) {
+cudaError_t launch_pr_phase(const TileSet& ts, int sweeps, int local_iters, cudaStream_t s, int sched) {
   if (ts.dims == 2) {
-    if (ts.pr_split && ts.TR == 16) return launch_t<2, 8, 1, true>(ts, sweeps, local_iters, s);
+    if (ts.pr_split && ts.TR == 16) return launch_t<2, 8, 1, true>(ts, sweeps, local_iters, s, sched);
     switch (ts.TR) {
-      case 8: return launch_t<2, 8, 1>(ts, sweeps, local_iters, s);
-      case 16: return launch_t<2, 16, 1>(ts, sweeps, local_iters, s);
+      case 8: return launch_t<2, 8, 1>(ts, sweeps, local_iters, s, sched);
+      case 16: return launch_t<2, 16, 1>(ts, sweeps, local_iters, s, sched);
       default: return cudaErrorInvalidValue;
     }
   }
-  if (ts.TY == 4 && ts.TZ == 4) return launch_t<3, 4, 4>(ts, sweeps, local_iters, s);
-  if (ts.TY == 4 && ts.TZ == 2) return launch_t<3, 4, 2>(ts, sweeps, local_iters, s);
-  if (ts.TY == 16 && ts.TZ == 1) return launch_t<3, 16, 1>(ts, sweeps, local_iters, s);
-  if (ts.TY == 8 && ts.TZ == 2) return launch_t<3, 8, 2>(ts, sweeps, local_iters, s);
-  if (ts.TY == 8 && ts.TZ == 1) return launch_t<3, 8, 1>(ts, sweeps, local_iters, s);
+  if (ts.TY == 4 && ts.TZ == 4) return launch_t<3, 4, 4>(ts, sweeps, local_iters, s, sched);
+  if (ts.TY == 4 && ts.TZ == 2) return launch_t<3, 4, 2>(ts, sweeps, local_iters, s, sched);
+  if (ts.TY == 16 && ts.TZ == 1) return launch_t<3, 16, 1>(ts, sweeps, local_iters, s, sched);
+  if (ts.TY == 8 && ts.TZ == 2) return launch_t<3, 8, 2>(ts, sweeps, local_iters, s, sched);
+  if (ts.TY == 8 && ts.TZ == 1) return launch_t<3, 8, 1>(ts, sweeps, local_iters, s, sched);
   return cudaErrorInvalidValue;
 }

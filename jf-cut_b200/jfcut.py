@@ -37,7 +37,7 @@ class JfcError(RuntimeError):
 class Params(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("tile_rows", "local_iters", "relabel_interval", "max_sweeps",
                                              "max_bfs_passes", "use_graph", "verbose", "relabel_interval_max",
-                                             "tile_depth", "pr_mode", "spin_limit", "relabel_cap")]
+                                             "tile_depth", "pr_mode", "spin_limit", "relabel_cap", "pr_sched")]
 
 
 class Model(ctypes.Structure):

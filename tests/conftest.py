@@ -103,13 +103,17 @@ def _default_schedule(request):
 
 
 # Schedules the parity tests run under: the default (32 x 8 tiles, 12 rounds
-# per visit, automatic relabel interval and relabel distance cap), 32 x 16
-# relabel tiles with push-relabel on their 32 x 8 halves, whole 32 x 16
-# push-relabel tiles, every relabel exact (no cap), and a cap of 2 (almost
-# every node starts unreachable, so the exact certifying relabel and the
-# uncapped continuation after it carry the solve).
+# per visit, automatic relabel interval, relabel distance cap and visit
+# scheduling), 32 x 16 relabel tiles with push-relabel on their 32 x 8
+# halves, whole 32 x 16 push-relabel tiles, every relabel exact (no cap), a
+# cap of 2 (almost every node starts unreachable, so the exact certifying
+# relabel and the uncapped continuation after it carry the solve), and the
+# two visit schedulers (checkerboard sweeps, asynchronous worklist) named
+# explicitly.
 SCHEDULES = {"default": {}, "rows16": dict(tile_rows=16), "whole16": dict(tile_rows=16, pr_mode=2),
-             "exact": dict(relabel_cap=-1), "cap2": dict(relabel_cap=2)}
+             "exact": dict(relabel_cap=-1), "cap2": dict(relabel_cap=2),
+             "sweeps": dict(pr_sched=1), "worklist": dict(pr_sched=2),
+             "rows16_sweeps": dict(tile_rows=16, pr_sched=1)}
 
 
 def use_schedule(ctx, name):

@@ -15,6 +15,7 @@ of the workload (replicas only: one grid does not shard without a per-sweep
 halo exchange), value = all ranks' nodes / max-over-ranks time.
 """
 import argparse
+import faulthandler
 import json
 import os
 import statistics
@@ -39,14 +40,16 @@ MODEL = dict(lambda_n=100, z_weight_pct=100, lambda_t=10, k_fg=5, k_bg=5, seed_c
 METRIC = "Mnodes/s to exact min-cut (plain, 2D 4-conn 15000x10000 RGB)"
 
 
-def pr_traffic_per_launch():
-    """DRAM bytes per push-relabel phase launch from the committed summary of
-    the ncu capture of this workload (under profiles/), or None."""
+def pr_traffic_per_visit():
+    """DRAM bytes per push-relabel tile visit from the committed summary of the
+    one-pass ncu capture of every push-relabel launch of a 4096x3072 solve
+    (under profiles/), or None; a full-size launch's traffic is this times its
+    visits (traffic grows with the visits: each reads and writes one tile)."""
     try:
-        with open(os.path.join(ROOT, "profiles", "k_pr_phase_traffic_15000x10000.md")) as f:
+        with open(os.path.join(ROOT, "profiles", "k_pr_phase_traffic_4096x3072.md")) as f:
             for line in f:
-                if line.startswith("traffic_bytes_per_launch:"):
-                    return int(line.split(":")[1])
+                if line.startswith("traffic_bytes_per_visit:"):
+                    return float(line.split(":")[1])
     except OSError:
         pass
     return None
@@ -545,6 +548,7 @@ def bench_edit4096(jfcut, torch, ctx, n_edits=100):
 
 
 def main():
+    faulthandler.enable()   # a crash reports every thread's Python stack on stderr
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -621,12 +625,13 @@ def main():
         l0 = jfcut.kernel_launches()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        visits, ms_pr, sweeps = 0, 0.0, 0
+        visits, ms_pr, sweeps, pr_phases = 0, 0.0, 0, 0
         agg = {"ms_total": 0.0, "ms_push_relabel": 0.0, "ms_global_relabel": 0.0, "ms_cut": 0.0,
                "global_relabels": 0, "bfs_passes": 0}
         for _ in range(args.steps):
             st = step_device()
             visits += st.tile_visits
+            pr_phases += st.pr_phases
             ms_pr += st.ms_push_relabel
             sweeps += st.sweeps
             for k in agg:
@@ -660,7 +665,7 @@ def main():
     bytes_per_visit = 32 * rows * 48 + (2 * 32 + 2 * rows) * 12
     achieved = visits * bytes_per_visit / (ms_pr / 1000.0) / 1e9 if ms_pr > 0 else 0.0
     peak, peak_kind = peaks()
-    pr_launches = int(agg["global_relabels"]) - args.steps    # one phase per relabel cycle
+    pr_launches = pr_phases   # push-relabel phase launches in the timed steps
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Mnodes/s", "n_gpus": world, "steps": args.steps,
@@ -680,14 +685,16 @@ def main():
             "clocks": clk,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": pr_traffic_per_launch() if (w, h) == (W_FULL, H_FULL) else None,
+                         "traffic": (pr_traffic_per_visit() * visits / max(1, pr_launches)
+                                     if pr_traffic_per_visit() else None),
                          "algorithmic_bytes_per_launch": visits * bytes_per_visit / max(1, pr_launches),
                          "launches": pr_launches,
                          "kernel": "k_pr_phase (push-relabel phases; %d B per tile visit algorithmic, %s peak; "
-                                   "traffic from the committed ncu capture of this workload)"
-                                   % (bytes_per_visit, peak_kind)},
+                                   "traffic: DRAM bytes per visit of the committed ncu capture of a 4096x3072 "
+                                   "solve times this workload's visits per launch)" % (bytes_per_visit, peak_kind)},
         }
         if world == 1 and not args.no_cpu_baseline:
+            print("bench: cpu baseline", file=sys.stderr, flush=True)
             line["cpu_baseline"] = cpu_baseline_bk(w, h, replica_seed(rank), flow_ref)
         extras = [] if world > 1 or args.extras == "none" else args.extras.split(",")
         vsize = tuple(int(v) for v in args.video_size.split("x"))
@@ -699,6 +706,7 @@ def main():
         with torch.cuda.stream(stream):
             for name in ("video", "batched", "edit4096", "serve", "fastcut"):
                 if name in extras:
+                    print("bench: section %s" % name, file=sys.stderr, flush=True)
                     t0 = time.perf_counter()
                     try:
                         line[name] = sections[name]()

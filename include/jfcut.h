@@ -106,6 +106,9 @@ typedef struct jfc_params {
                             1 = checkerboard parity sweeps with a grid barrier between colours,
                             2 = an asynchronous worklist with per-tile neighbour exclusion (no
                             barriers), 0 = automatic.  Same arithmetic, same results */
+  int local_iters_tail;  /* push/relabel rounds per visit once fewer than 1/256 of the tiles are
+                            active (the long-path tail of a solve, where excess has to cross
+                            whole tiles): 0 = automatic, < 0 = local_iters */
 } jfc_params;
 
 /* Capacity model (replaces computeCapacity / kmeans / computeExcessFlowLazy,
@@ -138,6 +141,7 @@ typedef struct jfc_stats {
   double ms_gr_first;     /* global relabel: dense first passes (device clock) */
   double ms_gr_frontier;  /* global relabel: frontier passes (device clock) */
   int used_graph;         /* 1 if the relabel cycles ran as CUDA graph launches */
+  int pr_phases;          /* push-relabel phase launches (one per relabel cycle) */
 } jfc_stats;
 
 typedef struct jfc_ctx jfc_ctx;

@@ -240,10 +240,9 @@ static size_t pin_need(const TileSet& ts) {
   return sizeof(DevCounters) + sizeof(long long) * 2 * (size_t)ts.ngrids + 64;
 }
 
-// pinned slot holding the sweep pairs of the next push-relabel phase, the
-// distance cap of the relabel after it and whether that relabel may skip
-// frozen tiles (after the read-back area); copied to the control block
-// (pr_sweeps, h_cap, skip_frozen) by the cycle itself
+// pinned slot holding the sweep pairs of the next push-relabel phase and the
+// distance cap of the relabel after it (after the read-back area); copied to
+// the control block (pr_sweeps, h_cap) by the cycle itself
 static int* pin_sweeps(jfc_ctx* ctx, const TileSet& ts) {
   return (int*)((char*)ctx->h_pin + (pin_need(ts) + 255) / 256 * 256);
 }
@@ -330,10 +329,9 @@ void tileset_drop_graphs(TileSet& ts) {
 static cudaError_t enqueue_cycle(TileSet& ts, const int* pin_sw, int local_iters, int max_passes, int sched,
                                  cudaStream_t s, void* pin) {
   cudaError_t e = cudaMemsetAsync(ts.d_ctr->ticket, 0, sizeof(ts.d_ctr->ticket), s);
-  static_assert(offsetof(DevCounters, h_cap) == offsetof(DevCounters, pr_sweeps) + sizeof(int) &&
-                    offsetof(DevCounters, skip_frozen) == offsetof(DevCounters, pr_sweeps) + 2 * sizeof(int),
-                "pr_sweeps, h_cap and skip_frozen are copied together");
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&ts.d_ctr->pr_sweeps, pin_sw, 3 * sizeof(int), cudaMemcpyHostToDevice, s);
+  static_assert(offsetof(DevCounters, h_cap) == offsetof(DevCounters, pr_sweeps) + sizeof(int),
+                "pr_sweeps and h_cap are copied together");
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&ts.d_ctr->pr_sweeps, pin_sw, 2 * sizeof(int), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = launch_pr_phase(ts, 0, local_iters, s, sched);
   if (e == cudaSuccess) e = enqueue_bfs(ts, false, max_passes, s, pin);
   return e;
@@ -378,24 +376,23 @@ static cudaGraphExec_t cycle_graph(TileSet& ts, const int* pin_sw, int local_ite
 
 // One relabel cycle, replayed from a graph when enabled; returns the outcome
 // of its global relabel.
-static int run_cycle(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, int interval, int h_cap, int& passes,
-                     std::vector<int>& active, int* sweeps_done, bool* used_graph) {
+static int run_cycle(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, int interval, int h_cap, int local_iters,
+                     int& passes, std::vector<int>& active, int* sweeps_done, bool* used_graph) {
   cudaStream_t s = ctx->stream;
   int rc = pin_reserve(ctx, pin_need_cycle(ts));
   if (rc) return rc;
   int* pin_sw = pin_sweeps(ctx, ts);
   pin_sw[0] = interval;   // the previous cycle's copies finished at its sync
   pin_sw[1] = h_cap;
-  pin_sw[2] = 1;          // within a solve, after its first relabel: frozen tiles are skipped
   const int sched = pr_sched_for(p);
-  cudaGraphExec_t x = p.use_graph ? cycle_graph(ts, pin_sw, p.local_iters, p.max_bfs_passes, sched, s, ctx->h_pin)
+  cudaGraphExec_t x = p.use_graph ? cycle_graph(ts, pin_sw, local_iters, p.max_bfs_passes, sched, s, ctx->h_pin)
                                   : nullptr;
   if (x) {
     JFC_CUDA(cudaGraphLaunch(x, s));
     jfc_note_launch(2);
     if (used_graph) *used_graph = true;
   } else {
-    JFC_CUDA(enqueue_cycle(ts, pin_sw, p.local_iters, p.max_bfs_passes, sched, s, ctx->h_pin));
+    JFC_CUDA(enqueue_cycle(ts, pin_sw, local_iters, p.max_bfs_passes, sched, s, ctx->h_pin));
   }
   JFC_CUDA(cudaStreamSynchronize(s));
   return finish_bfs(ts, false, ctx->h_pin, passes, &active, nullptr, sweeps_done);
@@ -441,7 +438,8 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   JFC_CUDA(launch_clear_counters(ts, s));
   // capped relabels while solving (the first one included), then one exact
   // relabel certifies the result
-  int h_cap = relabel_cap_for(p, ts.dims);
+  int h_cap = relabel_cap_for(p, ts.dims);   // cap of the next relabel
+  int last_cap = h_cap;                       // cap the last relabel ran with
   if (p.spin_limit > 0 || h_cap > 0)
     JFC_CUDA(launch_set_limits(ts, (unsigned long long)p.spin_limit, h_cap, s));
 #ifndef JFC_NO_PREPUSH
@@ -457,7 +455,14 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
 
   auto total = [&]() { long long t = 0; for (int v : active) t += v; return t; };
   const DevCounters* hc = (const DevCounters*)ctx->h_pin;
-  double prev_pr = 0.0, prev_gr = 0.0;
+  double prev_pr = 0.0, prev_gr = 0.0, prev_grf = 0.0;
+  if (p.verbose) {   // the first relabel's share
+    const DevCounters* c0 = (const DevCounters*)ctx->h_pin;
+    prev_gr = (c0->ns_gr_first + c0->ns_gr_frontier) * 1e-6;
+    prev_grf = c0->ns_gr_first * 1e-6;
+    fprintf(stderr, "{\"relabel\": 1, \"active_tiles\": %lld, \"ms_gr\": %.3f, \"ms_gr_dense\": %.3f}\n",
+            [&]() { long long t = 0; for (int v : active) t += v; return t; }(), prev_gr, prev_grf);
+  }
   int status = JFC_OK;
   // Adaptive schedule: while a large part of the grid is active, frequent
   // global relabels pay off; once only a sliver is active (long transport
@@ -468,6 +473,8 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   // its sweeps: the relabel is then the bottleneck and is amortised.
   const int interval0 = interval_for(p, ts.dims);
   int interval = interval0;
+  const int tail_iters = p.local_iters_tail > 0 ? p.local_iters_tail
+                         : p.local_iters_tail < 0 ? p.local_iters : std::min(2 * p.local_iters, 64);
   bool graphs = false;
   double fast_ms = 0.0;   // Fast-Cut iterations (event-timed: many small launches)
   unsigned long long last_pr = 0, last_gr = 0;
@@ -499,7 +506,13 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
       last_pr -= (unsigned long long)(fms * 1e6);   // the cost rule below sees the sweeps' time
       sw = 2 * interval;
     } else {
-      rc = run_cycle(ctx, ts, p, interval, h_cap, st.bfs_passes, active, &sw, &graphs);
+      // the long-path tail (a sliver of the tiles active): longer visits, so
+      // excess crosses a whole tile per visit instead of per several sweeps
+      const bool tail = total() * 256 < (long long)ts.ntiles;
+      const int li = tail ? tail_iters : p.local_iters;
+      rc = run_cycle(ctx, ts, p, interval, h_cap, li, st.bfs_passes, active, &sw, &graphs);
+      last_cap = h_cap;
+      ++st.pr_phases;
       if (rc) return rc;
     }
     st.sweeps += sw;
@@ -517,17 +530,21 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
     if (p.verbose) {
       hc = (const DevCounters*)ctx->h_pin;
       const double pr = hc->ns_pr * 1e-6, gr = (hc->ns_gr_first + hc->ns_gr_frontier) * 1e-6;
-      fprintf(stderr, "{\"relabel\": %d, \"sweeps\": %d, \"active_tiles\": %lld, \"ms_pr\": %.3f, \"ms_gr\": %.3f}\n",
-              st.global_relabels, st.sweeps, total(), pr - prev_pr, gr - prev_gr);
+      const double grf = hc->ns_gr_first * 1e-6;
+      fprintf(stderr, "{\"relabel\": %d, \"sweeps\": %d, \"active_tiles\": %lld, \"ms_pr\": %.3f, \"ms_gr\": %.3f, "
+                      "\"ms_gr_dense\": %.3f}\n",
+              st.global_relabels, st.sweeps, total(), pr - prev_pr, gr - prev_gr, grf - prev_grf);
       prev_pr = pr;
       prev_gr = gr;
+      prev_grf = grf;
     }
   }
   // no active tile under the cap: one exact relabel decides.  Excess it finds
   // reachable (farther than the cap from every deficit) keeps the solve going
   // with exact relabels; none means the preflow is maximum.
-  if (status != JFC_OK || h_cap == 0) break;
+  if (status != JFC_OK || last_cap == 0) break;
   h_cap = 0;
+  last_cap = 0;
   JFC_CUDA(launch_set_limits(ts, (unsigned long long)p.spin_limit, 0, s));
   rc = engine_bfs(ctx, ts, p, false, st.bfs_passes, &active, nullptr, nullptr);
   if (rc) return rc;

@@ -24,14 +24,6 @@
 #define JFC_PAD_Z3 4        // 3D z padding (tile depths 1, 2, 4)
 #define JFC_MAX_K 32        // k-means clusters per class
 #define JFC_TQ 65536        // t-link probability quantisation
-// Tile activity byte: the dense relabel pass gave the tile no finite height
-// (no deficit in it, none across a residual arc from its halo) and no later
-// relabel visit lowered one.  Push-relabel never enters such a tile (its
-// nodes are inactive and nothing pushes into an unreachable node) and
-// deficits never appear, so its excess, arcs, heights and arc bytes stay as
-// they are and the dense pass of a later relabel in the same solve would give
-// the same result: that pass skips it.
-#define JFC_ACT_FROZEN 4u
 
 // Device-side descriptor of one grid instance.
 struct GridDev {
@@ -39,6 +31,8 @@ struct GridDev {
   int pitch, Hp, Dp;
   int tiles_x, tiles_y, tiles_z;
   int tile_base;             // global id of this grid's first tile
+  int h_cap;                 // distance cap of this grid's global relabels (0: the tile set's, h_cap
+                             // of its control block)
   long long plane;           // pitch * Hp * Dp
   int* e;
   int* h;
@@ -61,8 +55,7 @@ struct DevCounters {
   int sweeps_done;           // sweeps run by the last push-relabel phase
   int pr_sweeps;             // sweep pairs of the next phase when launched with sweeps <= 0
   int h_cap;                 // global relabels: distances >= h_cap count as unreachable (0: no cap)
-  int skip_frozen;           // global relabels: the dense pass skips frozen tiles (JFC_ACT_FROZEN);
-                             // pr_sweeps, h_cap, skip_frozen: a relabel cycle copies them at once
+                             // (pr_sweeps and h_cap: a relabel cycle copies both at once)
   int fast_moved;            // a Fast-Cut push moved flow (comparison mode)
   unsigned long long visits; // push-relabel tile visits
   unsigned long long bfs_visits;
@@ -98,7 +91,7 @@ struct TileSet {
   int* d_flag_bfs[2] = {nullptr, nullptr};  // [buffer][ntiles] tile waits in a BFS frontier
   int* d_q_bfs[2] = {nullptr, nullptr};     // [buffer] BFS frontiers
   uint8_t* d_act = nullptr;          // [ntiles] bits 0-1: tile (half) held an active node at its last
-                                     // relabel visit; JFC_ACT_FROZEN: see below
+                                     // relabel visit
   int* d_grid_active = nullptr;      // [ngrids] active tiles after global relabel
   unsigned long long* d_pr_ring = nullptr;  // [work items] push-relabel worklist ring (null: sweeps only)
   int* d_pr_lock = nullptr;          // [work items] a visit of the item is in progress

@@ -59,6 +59,10 @@ __device__ __forceinline__ int height_cap(const DevCounters* ctr) {
   const int v = vload(&ctr->h_cap);
   return v > 0 ? v : JFC_INF;
 }
+// The cap for grid g: its own when set, else the tile set's.
+__device__ __forceinline__ int cap_of(const GridDev& g, const DevCounters* ctr) {
+  return g.h_cap > 0 ? g.h_cap : height_cap(ctr);
+}
 
 // Device-wide nanosecond clock (phase timing of the persistent kernels).
 __device__ __forceinline__ unsigned long long global_ns() {

@@ -489,7 +489,7 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
     if (arcs & jfc::A_ZP) m = min(m, s.h[hi + T::SZ]);
     if (arcs & jfc::A_ZM) m = min(m, s.h[hi - T::SZ]);
   }
-  const int cap = jfc::height_cap(ts.d_ctr);
+  const int cap = jfc::cap_of(g, ts.d_ctr);
   const bool need = __syncthreads_or(m + 1 < hstart && m + 1 < cap);
   const bool converged = need ? jfc::relax_cta<DIMS, TY, TZ>(s.h, s.arc, 16) : true;
   // distances at or above the cap stay unreachable (every stored height is
@@ -535,7 +535,7 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
     else jfc::warp_append(want, nb, Q.flags, Q.q, Q.qn);
     if (t == 0) {
       const int old = ((fresh ? __ldcg(ts.d_act + tid) : ts.d_act[tid]) & 3u) != 0 ? 1 : 0;
-      ts.d_act[tid] = (uint8_t)((act_lo ? 1 : 0) | (act_hi ? 2 : 0));   // a visited tile is not frozen
+      ts.d_act[tid] = (uint8_t)((act_lo ? 1 : 0) | (act_hi ? 2 : 0));
       if (ti.x != cur_grid) {
         if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
         delta = 0;
@@ -559,29 +559,32 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
   using D = Dirs<DIMS>;
   constexpr int R = TY * TZ;
   const int lane = threadIdx.x & 31;
-  // a frozen tile would get the same (all unreachable) result again
-#ifndef JFC_NO_FROZEN_SKIP
-  if (jfc::vload(&ts.d_ctr->skip_frozen) && (ts.d_act[tid] & JFC_ACT_FROZEN)) return;
-#endif
   const int4 ti = ts.d_info[tid];
   const GridDev& g = ts.d_desc[ti.x];
   const Addr a = make_addr<DIMS, TY, TZ>(g, ti, lane);
   unsigned AXP[R], AXM[R], AYP[R], AYM[R], AZP[DIMS == 3 ? R : 1], AZM[DIMS == 3 ? R : 1];
   unsigned DEF[R], POS[R], V[R], F[R];
+  // each node as one byte (arc bits, bit 6 e < 0, bit 7 e > 0); the row
+  // masks come from it
 #pragma unroll
   for (int i = 0; i < R; ++i) {
     const long long n = roff<TY>(a, i);
     const int e = g.e[n];
-    AXP[i] = __ballot_sync(FULL, g.r[D::XP][n] > 0);
-    AXM[i] = __ballot_sync(FULL, g.r[D::XM][n] > 0);
-    AYP[i] = __ballot_sync(FULL, g.r[D::YP][n] > 0);
-    AYM[i] = __ballot_sync(FULL, g.r[D::YM][n] > 0);
+    unsigned b = (g.r[D::XP][n] > 0 ? jfc::A_XP : 0u) | (g.r[D::YP][n] > 0 ? jfc::A_YP : 0u) |
+                 (g.r[D::YM][n] > 0 ? jfc::A_YM : 0u) | (g.r[D::XM][n] > 0 ? jfc::A_XM : 0u) |
+                 (e < 0 ? 64u : 0u) | (e > 0 ? 128u : 0u);
+    if constexpr (DIMS == 3)
+      b |= (g.r[D::ZP][n] > 0 ? jfc::A_ZP : 0u) | (g.r[D::ZM][n] > 0 ? jfc::A_ZM : 0u);
+    AXP[i] = __ballot_sync(FULL, b & jfc::A_XP);
+    AXM[i] = __ballot_sync(FULL, b & jfc::A_XM);
+    AYP[i] = __ballot_sync(FULL, b & jfc::A_YP);
+    AYM[i] = __ballot_sync(FULL, b & jfc::A_YM);
     if constexpr (DIMS == 3) {
-      AZP[i] = __ballot_sync(FULL, g.r[D::ZP][n] > 0);
-      AZM[i] = __ballot_sync(FULL, g.r[D::ZM][n] > 0);
+      AZP[i] = __ballot_sync(FULL, b & jfc::A_ZP);
+      AZM[i] = __ballot_sync(FULL, b & jfc::A_ZM);
     }
-    DEF[i] = __ballot_sync(FULL, e < 0);
-    POS[i] = __ballot_sync(FULL, e > 0);
+    DEF[i] = __ballot_sync(FULL, b & 64u);
+    POS[i] = __ballot_sync(FULL, b & 128u);
     V[i] = DEF[i];
     F[i] = DEF[i];
   }
@@ -624,13 +627,13 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
     }
   }
   // the frontier passes read one byte per node instead of e and the residual
-  // planes: bits 0-5 residual arcs (jfc::A_*), bit 7 e > 0 (the label plane
-  // is free until the cut BFS writes it)
+  // planes: bits 0-5 residual arcs (jfc::A_*), bit 6 e < 0, bit 7 e > 0 (the
+  // label plane is free until the cut BFS writes it)
 #pragma unroll
   for (int i = 0; i < R; ++i) {
     unsigned b = ((AXP[i] >> lane) & 1u) * jfc::A_XP | ((AYP[i] >> lane) & 1u) * jfc::A_YP |
                  ((AYM[i] >> lane) & 1u) * jfc::A_YM | ((AXM[i] >> lane) & 1u) * jfc::A_XM |
-                 ((POS[i] >> lane) & 1u) * 128u;
+                 ((DEF[i] >> lane) & 1u) * 64u | ((POS[i] >> lane) & 1u) * 128u;
     if constexpr (DIMS == 3) b |= ((AZP[i] >> lane) & 1u) * jfc::A_ZP | ((AZM[i] >> lane) & 1u) * jfc::A_ZM;
     g.label[roff<TY>(a, i)] = (uint8_t)b;
   }
@@ -639,7 +642,7 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
   for (int i = 0; i < R; ++i) h[i] = ((DEF[i] >> lane) & 1u) ? 0 : JFC_INF;
   // level-synchronous expansion: u reaches level d+1 through an arc to a level-d node
   // (levels at or above the relabel's distance cap stay unreachable)
-  const int dmax = min(32 * R, jfc::height_cap(ts.d_ctr) - 1);
+  const int dmax = min(32 * R, jfc::cap_of(g, ts.d_ctr) - 1);
   for (int d = 0; d < dmax; ++d) {
     unsigned any = 0;
     unsigned N[R];
@@ -665,10 +668,9 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
       if ((N[i] >> lane) & 1u) h[i] = d + 1;
     }
   }
-  unsigned rows_fin = 0, c0 = 0, c31 = 0, act = 0, act_hi = 0, any_finite = 0;
+  unsigned rows_fin = 0, c0 = 0, c31 = 0, act = 0, act_hi = 0;
 #pragma unroll
   for (int i = 0; i < R; ++i) {
-    any_finite |= V[i];
     g.h[roff<TY>(a, i)] = h[i];
     const unsigned fin = V[i] & ~DEF[i];   // finite and above 0: news for the neighbours
     if (fin) rows_fin |= 1u << i;
@@ -680,7 +682,7 @@ __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, c
   }
   if (lane == 0) {
     const int old = 0;
-    ts.d_act[tid] = (uint8_t)((act ? 1 : 0) | (act_hi ? 2 : 0) | (any_finite ? 0u : JFC_ACT_FROZEN));
+    ts.d_act[tid] = (uint8_t)((act ? 1 : 0) | (act_hi ? 2 : 0));
     act |= act_hi;
     if (ti.x != cur_grid) {
       if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
@@ -782,7 +784,7 @@ __device__ __forceinline__ void relabel_frontier_warp(const TileSet& ts, int tid
   for (int i = 0; i < R; ++i) F[i] = 0u;
   unsigned rows_changed = 0, c0 = 0, c31 = 0;
   bool again = false;
-  const int cap = jfc::height_cap(ts.d_ctr);   // levels at or above it stay unreachable
+  const int cap = jfc::cap_of(g, ts.d_ctr);   // levels at or above it stay unreachable
   int d = next_level(-1);
   for (int level = 0; d < cap; ++level) {
     if (level >= kMaxLevels) { again = true; break; }
@@ -823,13 +825,21 @@ __device__ __forceinline__ void relabel_frontier_warp(const TileSet& ts, int tid
     }
     d = any ? d + 1 : next_level(d);
   }
-  bool act = false;
+  // activity per 8-row half of a 2D 32x16 tile (bit 0 rows 0-7, bit 1 rows
+  // 8-15: the push-relabel work items of split tile sets), else bit 0
+  bool act_lo = false, act_hi = false;
 #pragma unroll
-  for (int i = 0; i < R; ++i) act |= ((posm >> i) & 1u) && hv[i] < JFC_INF;
-  act = __any_sync(FULL, act);
+  for (int i = 0; i < R; ++i) {
+    const bool live = ((posm >> i) & 1u) && hv[i] < JFC_INF;
+    if (DIMS == 2 && TY == 16 && i >= 8) act_hi |= live;
+    else act_lo |= live;
+  }
+  act_lo = __any_sync(FULL, act_lo);
+  act_hi = __any_sync(FULL, act_hi);
+  const bool act = act_lo || act_hi;
   if (lane == 0) {
     const int old = (ts.d_act[tid] & 3u) != 0 ? 1 : 0;
-    ts.d_act[tid] = act ? 1 : 0;   // a visited tile is not frozen
+    ts.d_act[tid] = (uint8_t)((act_lo ? 1 : 0) | (act_hi ? 2 : 0));
     if (ti.x != cur_grid) {
       if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
       delta = 0;
@@ -984,9 +994,10 @@ __global__ void __launch_bounds__(256, JFC_RELABEL_WARP_MINB) k_relabel_warp(Til
 // queues the tile for a full visit only when some residual arc u -> v out of
 // the tile has h(v) + 1 < h(u).
 template <int TY>
-__device__ __forceinline__ bool border_improvable(const TileSet& ts, int tid, int lane, int cap) {
+__device__ __forceinline__ bool border_improvable(const TileSet& ts, int tid, int lane) {
   const int4 ti = ts.d_info[tid];
   const GridDev& g = ts.d_desc[ti.x];
+  const int cap = jfc::cap_of(g, ts.d_ctr);
   const long long pitch = g.pitch;
   const int x0 = ti.y * 32, y0 = ti.z * TY;
   const long long base = (long long)x0 + (long long)y0 * pitch;
@@ -1042,7 +1053,7 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
         if ((int)k >= n) break;
         const int tt = queue[k];
         if (lane == 0) fcur[tt] = 0;
-        const bool imp = border_improvable<TY>(ts, tt, lane, jfc::height_cap(ctr));
+        const bool imp = border_improvable<TY>(ts, tt, lane);
         jfc::warp_append(imp && lane == 0, tt, Q.flags, Q.q, Q.qn);
       }
     } else {
@@ -1146,7 +1157,9 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
       if (threadIdx.x < 32) ++visits;
     }
   }
-  if (threadIdx.x == 0 && delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
+  // per-grid activity deltas: thread 0 holds the CTA visits', lane 0 of
+  // each warp the warp visits'
+  if (lane == 0 && delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
   // refill the push-relabel queues (buffer 0 of each parity) from the
   // active-tile flags
   if (ok) ok = jfc::grid_sync(ctr, [&]() {

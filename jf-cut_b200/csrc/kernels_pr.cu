@@ -283,7 +283,10 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
   const bool active = __syncthreads_or((e1 > 0) & (h1 < JFC_INF));
   // flow crossed face f only toward an item inside the grid (arcs leaving
   // the grid are zero)
-  if (t < 6) s.q_nb[t] = s.face[t] ? face_item<DIMS, TY, TZ, SPLIT>(ts, tid, t) : -1;
+  if (t < 6) {
+    const int nb = s.face[t] ? face_item<DIMS, TY, TZ, SPLIT>(ts, tid, t) : -1;
+    s.q_nb[t] = nb;
+  }
   if (t == 0) s.active = active ? 1 : 0;
   __syncthreads();
   JFC_PCLK(ts.d_ctr, 3);

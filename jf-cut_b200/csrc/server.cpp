@@ -72,6 +72,10 @@ struct Session {
   bool has_last = false;
   long long sweeps = 0;             // sweeps of the current request
   bool cancel = false, close = false;
+  int lane_refs = 0;                // lane entries that hold this session (joining, solving, or
+                                    // done but not yet removed; a finished session can be
+                                    // re-admitted before its old entry leaves).  Guarded by mu; a
+                                    // closed session is freed only once none is left
 };
 
 }  // namespace
@@ -274,7 +278,7 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
         }
         if (m.done) {
           changed[k] = true;
-          if (m.s->close) L.freeing.push_back(m.s);
+          if (--m.s->lane_refs == 0 && m.s->close) L.freeing.push_back(m.s);
           continue;
         }
         keep.push_back(m);
@@ -325,6 +329,15 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
   for (int k = 0; k < 2; ++k) {
     std::vector<size_t> conv;
     for (size_t i = 0; i < L.mem[k].size(); ++i) {
+      GridDev& gd = L.mem[k][i].s->G->g;
+      if (L.active[k][i] == 0 && gd.h_cap > 0) {
+        // no active tile under the cap: the grid's next relabel is exact and
+        // decides (excess farther than the cap keeps it solving)
+        gd.h_cap = 0;
+        const cudaError_t e = cudaMemsetAsync(&L.ts[k].d_desc[i].h_cap, 0, sizeof(int), ctx->stream);
+        if (e != cudaSuccess) return cuda_status(e, "relabel cap");
+        continue;
+      }
       if (L.active[k][i] == 0) conv.push_back(i);
       else if (L.mem[k][i].s->sweeps >= p.max_sweeps) conv.push_back(i);
       else still += L.active[k][i];
@@ -403,11 +416,12 @@ void solver_loop(jfc_server* S) {
         if (s->cancel || s->reqs.empty()) {
           cancel_all(S, s, now);
           s->phase = IDLE;
-          if (s->close) frees.push_back(s);
+          if (s->close && s->lane_refs == 0) frees.push_back(s);   // else its lane frees it
           S->cv_done.notify_all();
           continue;
         }
         s->phase = SOLVING;
+        ++s->lane_refs;
         if (!s->reqs.front().cold) s->reqs.front().t_admit = now;
         admitted.push_back(s);
         --slots;
@@ -428,12 +442,17 @@ void solver_loop(jfc_server* S) {
         if (!r.cold) rc = jfc_graph_edit_seeds(s->G, r.idx.data(), r.seed.data(), r.idx.size());
         if (rc != JFC_OK) {
           std::lock_guard<std::mutex> lk(S->mu);
+          --s->lane_refs;   // admitted, but it joins no lane
           finish_front(S, s, rc, 0, Clock::now());
           s->phase = s->reqs.empty() ? IDLE : READY;
           if (!s->reqs.empty()) S->ready_q.push_back(s->sid);
+          else if (s->close && s->lane_refs == 0) S->to_free.push_back(s);   // closed meanwhile
           S->cv_done.notify_all();
           continue;
         }
+        // capped relabels while the request solves (the plain solve's
+        // schedule); dropped for the grid once it has no active tile left
+        s->G->g.h_cap = relabel_cap_for(S->params, s->dims);
         lanes[r.cold ? 1 : 0].joining.push_back(s);
       }
     }
@@ -668,12 +687,14 @@ int jfc_server_close(jfc_server* S, int sid) {
     S->build_q.erase(std::remove(S->build_q.begin(), S->build_q.end(), sid), S->build_q.end());
     cancel_all(S, s, now);
     S->sessions.erase(sid);   // nothing on the device yet
-  } else if (s->phase == IDLE || s->phase == DEAD) {
+  } else if ((s->phase == IDLE || s->phase == DEAD) && s->lane_refs == 0) {
     cancel_all(S, s, now);
     S->to_free.push_back(s);  // freed by the solver between launches
     S->cv_work.notify_all();
   }
-  // READY / BUILDING / SOLVING: the owner thread finishes and frees it
+  // READY / BUILDING / SOLVING, or a finished request whose lane still holds
+  // the session: the owner thread finishes and frees it (a lane drops its
+  // done members at its next membership change and frees the closed ones)
   S->cv_done.notify_all();
   return JFC_OK;
 }

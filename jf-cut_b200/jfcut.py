@@ -37,7 +37,8 @@ class JfcError(RuntimeError):
 class Params(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("tile_rows", "local_iters", "relabel_interval", "max_sweeps",
                                              "max_bfs_passes", "use_graph", "verbose", "relabel_interval_max",
-                                             "tile_depth", "pr_mode", "spin_limit", "relabel_cap", "pr_sched")]
+                                             "tile_depth", "pr_mode", "spin_limit", "relabel_cap", "pr_sched",
+                                             "local_iters_tail")]
 
 
 class Model(ctypes.Structure):
@@ -51,7 +52,8 @@ class Stats(ctypes.Structure):
                 ("source_nodes", ctypes.c_longlong), ("ms_total", ctypes.c_double), ("ms_build", ctypes.c_double),
                 ("ms_push_relabel", ctypes.c_double), ("ms_global_relabel", ctypes.c_double),
                 ("ms_cut", ctypes.c_double), ("pr_rounds", ctypes.c_longlong), ("bfs_visits", ctypes.c_longlong),
-                ("ms_gr_first", ctypes.c_double), ("ms_gr_frontier", ctypes.c_double), ("used_graph", ctypes.c_int)]
+                ("ms_gr_first", ctypes.c_double), ("ms_gr_frontier", ctypes.c_double), ("used_graph", ctypes.c_int),
+                ("pr_phases", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -219,3 +219,49 @@ def test_cancel_and_close(ctx):
         assert st["sessions"] == 0 and st["used"] == 0
     finally:
         srv.close()
+
+
+def test_close_right_after_result_while_others_solve(ctx):
+    """A session closed the moment its last result arrives, while it is still
+    held by its lane and other sessions keep solving, is freed once (no use
+    after free, no leak); results stay the oracle's."""
+    reqs = make_requests(23, 20, 4, lo=40, hi=260)
+    srv = jfcut.Server(ctx, 0, max_slots=64)
+    results, errors = {}, []
+    lock = threading.Lock()
+
+    def client(i):
+        img, seeds, pf, model = reqs[i]
+        try:
+            sid = srv.submit(img, seeds, pf, model)
+            info = srv.wait(sid, 120000)
+            ed = strokes(seeds.shape, 300 + i, 1 + i % 3)
+            for idx, ns in ed:
+                srv.edit(sid, idx, ns)
+                info = srv.wait(sid, 120000)
+            srv.close_session(sid)          # right after the result
+            with lock:
+                results[i] = (info.status, info.flow, ed)
+        except Exception as ex:
+            with lock:
+                errors.append(repr(ex))
+
+    try:
+        threads = [threading.Thread(target=client, args=(i,)) for i in range(len(reqs))]
+        for t in threads:
+            t.start()
+            time.sleep(0.002)
+        for t in threads:
+            t.join()
+        assert not errors, errors[:3]
+        for i, (status, flow, ed) in results.items():
+            img, seeds, pf, model = reqs[i]
+            assert status == 0
+            assert flow == cpu_oracle(img, seeds, pf, model, ed)[0]
+        deadline = time.time() + 20
+        while srv.stats()["sessions"] and time.time() < deadline:
+            time.sleep(0.01)
+        st = srv.stats()
+        assert st["sessions"] == 0 and st["used"] == 0
+    finally:
+        srv.close()

@@ -243,7 +243,7 @@ void fail_lane(jfc_server* S, Lane& L, int rc) {
 // One relabel cycle of a lane: push-relabel phase over its members, then
 // membership (leave / join), then one global relabel over the re-formed set,
 // then the cut of every converged grid.  Returns a status (device errors).
-int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
+int lane_cycle(jfc_server* S, Lane& L, int lane_id, int max_interval = 1 << 30) {
   jfc_ctx* ctx = S->solve_ctx;
   const jfc_params& p = S->params;
   const Clock::time_point t_start = Clock::now();
@@ -256,7 +256,7 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
       if (!L.mem[k][i].done) a += L.active[k][i];
     if (a == 0) continue;
     cudaMemsetAsync(L.ts[k].d_ctr->ticket, 0, sizeof(L.ts[k].d_ctr->ticket), ctx->stream);
-    const cudaError_t e = launch_pr_phase(L.ts[k], L.interval, p.local_iters, ctx->stream);
+    const cudaError_t e = launch_pr_phase(L.ts[k], std::min(L.interval, max_interval), p.local_iters, ctx->stream);
     if (e != cudaSuccess) return cuda_status(e, "push-relabel phase");
     ran_pr[k] = true;
   }
@@ -383,7 +383,8 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
     auto ms = [](Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
     fprintf(stderr, "{\"lane\": \"%s\", \"members\": %zu, \"active_tiles\": %lld, \"tiles\": %lld, \"interval\": %d, "
                     "\"ms_phase_membership\": %.3f, \"ms_form_relabel\": %.3f, \"ms_cut\": %.3f}\n",
-            lane_id == 0 ? "interactive" : "bulk", L.mem[0].size() + L.mem[1].size(), still, nt, L.interval,
+            lane_id == 0 ? "interactive" : lane_id == 1 ? "interactive-large" : "bulk",
+            L.mem[0].size() + L.mem[1].size(), still, nt, L.interval,
             ms(t_start, t_form), ms(t_form, t_relabel), ms(t_relabel, t_end));
   }
   if (still > 0 && still * 256 < nt) L.interval = std::min(L.interval * 2, p.relabel_interval_max);
@@ -394,15 +395,30 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id) {
 void solver_loop(jfc_server* S) {
   cudaSetDevice(S->device);
   const jfc_params& p = S->params;
-  Lane lanes[2];                    // [0] interactive (warm edits), [1] bulk (cold)
-  lanes[0].interval = lanes[1].interval = interval_for(p, 2);
+  // [0] interactive: warm edits of 2D grids up to 4096^2 nodes; [1] interactive
+  // large: warm edits of volumes and larger images (their relabels take tens
+  // of milliseconds, which an edit of a small image should not wait for);
+  // [2] bulk: cold requests
+  Lane lanes[3];
+  constexpr int kSmall = 0, kLarge = 1, kBulk = 2;
+  for (Lane& L : lanes) L.interval = interval_for(p, 2);
+  constexpr long long kSmallEditNodes = 4096ll * 4096ll;
+  constexpr int kLargeEvery = 4;            // one large-edit cycle per this many small-edit cycles
   constexpr int kInteractiveCycles = 16;   // interactive cycles per bulk cycle, at most
+  // The bulk lane's size bounds how long one bulk cycle (a push-relabel phase
+  // and a relabel over every member) keeps a warm edit waiting: cold requests
+  // join while the lane holds fewer nodes than this (always at least one),
+  // and its push-relabel phases run at most kBulkPairsBusy sweep pairs while
+  // the interactive lane has work.
+  constexpr long long kBulkNodes = 1ll << 28;
+  constexpr int kBulkPairsBusy = 2;
+  auto nodes_of = [](const Session* s) { return (long long)s->w * s->h * s->d; };
   for (;;) {
     // admission: requests waiting for a slot join their lane at its next relabel
     std::vector<Session*> admitted, frees;
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      if (lanes[0].empty() && lanes[1].empty())
+      if (lanes[0].empty() && lanes[1].empty() && lanes[2].empty())
         S->cv_work.wait(lk, [&] { return S->stop || !S->ready_q.empty() || !S->to_free.empty(); });
       if (S->stop) break;
       const Clock::time_point now = Clock::now();
@@ -410,9 +426,26 @@ void solver_loop(jfc_server* S) {
       int members = 0;
       for (Lane& L : lanes) members += (int)(L.mem[0].size() + L.mem[1].size() + L.joining.size());
       int slots = S->max_slots - members;
+      long long bulk_nodes = 0;
+      for (int k = 0; k < 2; ++k)
+        for (const Member& m : lanes[kBulk].mem[k])
+          if (!m.done) bulk_nodes += nodes_of(m.s);
+      for (const Session* s : lanes[kBulk].joining) bulk_nodes += nodes_of(s);
+      // in queue order; a cold request that would overfill the bulk lane
+      // keeps its place (and the cold ones behind it theirs), edits go ahead
+      std::deque<int> keep;
+      bool bulk_full = false;
       while (slots > 0 && !S->ready_q.empty()) {
         Session* s = S->sessions.at(S->ready_q.front()).get();
+        const int sid = S->ready_q.front();
         S->ready_q.pop_front();
+        const bool cold = !s->reqs.empty() && s->reqs.front().cold && !s->cancel;
+        if (cold && (bulk_full || (bulk_nodes > 0 && bulk_nodes + nodes_of(s) > kBulkNodes))) {
+          bulk_full = true;
+          keep.push_back(sid);
+          continue;
+        }
+        if (cold) bulk_nodes += nodes_of(s);
         if (s->cancel || s->reqs.empty()) {
           cancel_all(S, s, now);
           s->phase = IDLE;
@@ -425,6 +458,10 @@ void solver_loop(jfc_server* S) {
         if (!s->reqs.front().cold) s->reqs.front().t_admit = now;
         admitted.push_back(s);
         --slots;
+      }
+      while (!keep.empty()) {   // back to the front, in order
+        S->ready_q.push_front(keep.back());
+        keep.pop_back();
       }
       ++S->loops;
     }
@@ -453,7 +490,8 @@ void solver_loop(jfc_server* S) {
         // capped relabels while the request solves (the plain solve's
         // schedule); dropped for the grid once it has no active tile left
         s->G->g.h_cap = relabel_cap_for(S->params, s->dims);
-        lanes[r.cold ? 1 : 0].joining.push_back(s);
+        const bool small = s->dims == 2 && nodes_of(s) <= kSmallEditNodes;
+        lanes[r.cold ? kBulk : small ? kSmall : kLarge].joining.push_back(s);
       }
     }
     {
@@ -464,18 +502,32 @@ void solver_loop(jfc_server* S) {
       S->peak_solving = std::max(S->peak_solving, solving);
     }
     // interactive lane first (until it drains, bounded), then one bulk cycle
-    for (int c = 0; c < kInteractiveCycles && !lanes[0].empty(); ++c) {
-      const int rc = lane_cycle(S, lanes[0], 0);
-      if (rc) { fail_lane(S, lanes[0], rc); fail_lane(S, lanes[1], rc); return; }
-      if (lanes[0].active_tiles() == 0 && lanes[0].joining.empty()) {
+    auto fail_all = [&](int rc) { for (Lane& L : lanes) fail_lane(S, L, rc); };
+    // edits first (until they drain, bounded): small-edit cycles, with a
+    // large-edit cycle every kLargeEvery of them (every cycle when no small
+    // edit waits); then one bulk cycle, short while any edit waits
+    for (int c = 0; c < kInteractiveCycles; ++c) {
+      const bool small = !lanes[kSmall].empty(), large = !lanes[kLarge].empty();
+      if (!small && !large) break;
+      if (small) {
+        const int rc = lane_cycle(S, lanes[kSmall], kSmall);
+        if (rc) { fail_all(rc); return; }
+      }
+      if (large && (!small || c % kLargeEvery == kLargeEvery - 1)) {
+        const int rc = lane_cycle(S, lanes[kLarge], kLarge, small ? kBulkPairsBusy : 1 << 30);
+        if (rc) { fail_all(rc); return; }
+      }
+      if (lanes[kSmall].active_tiles() == 0 && lanes[kSmall].joining.empty() &&
+          lanes[kLarge].active_tiles() == 0 && lanes[kLarge].joining.empty()) {
         // converged members leave at the next cycle; run it now only if
         // someone is waiting for a slot
         break;
       }
     }
-    if (!lanes[1].empty()) {
-      const int rc = lane_cycle(S, lanes[1], 1);
-      if (rc) { fail_lane(S, lanes[0], rc); fail_lane(S, lanes[1], rc); return; }
+    if (!lanes[kBulk].empty()) {
+      const bool busy = !lanes[kSmall].empty() || !lanes[kLarge].empty();
+      const int rc = lane_cycle(S, lanes[kBulk], kBulk, busy ? kBulkPairsBusy : 1 << 30);
+      if (rc) { fail_all(rc); return; }
     }
   }
   for (Lane& L : lanes)

@@ -20,6 +20,8 @@
 // instead of returning a non-converged cut.
 #include "engine.h"
 
+#include <cuda.h>   // CUtensorMap and the tensor-map encode function's types
+
 #include <algorithm>
 #include <atomic>
 #include <cstddef>
@@ -92,6 +94,60 @@ void tileset_free(TileSet& ts) {
   ts = TileSet();
 }
 
+// Tensor maps of one grid for the push-relabel staging (two CUtensorMap).
+constexpr size_t kTmapBytes = 2 * sizeof(CUtensorMap);
+// 0: visits load their tiles with ordinary loads (a comparison build)
+#ifndef JFC_PR_TMA
+#define JFC_PR_TMA 1
+#endif
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// The driver's tiled tensor-map encoder (resolved once; null when absent).
+static EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = []() -> EncodeTiledFn {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// Encode grid g's staging maps for visits of 32 x ty x tz nodes into out[2]:
+//  [0] the planes {e, h, r[0..K-1]} as one 4D tensor {pitch, Hp, Dp, planes},
+//      box {32, ty, tz, planes};
+//  [1] the h plane {pitch, Hp, Dp}, box {40, ty + 2, tz + 2 (1 in 2D)} (the
+//      tile and its one-cell halo, starting 4 columns left of the tile).
+// Returns false when the planes are not one evenly spaced run or a map is
+// refused; the tile set then stages with ordinary loads.
+static bool encode_pr_maps(const GridDev& g, int ty, int tz, CUtensorMap* out) {
+  const EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  const int K = g.dims == 2 ? 4 : 6;
+  const long long pb = (long long)((const char*)g.h - (const char*)g.e);
+  if (pb < g.plane * 4 || pb % 16 || (size_t)g.e % 16 || (g.pitch * 4) % 16) return false;
+  for (int k = 0; k < K; ++k)
+    if ((const char*)g.r[k] != (const char*)g.e + (2 + k) * pb) return false;
+  const cuuint64_t row = (cuuint64_t)g.pitch * 4, slab = row * (cuuint64_t)g.Hp;
+  const cuuint64_t dims4[4] = {(cuuint64_t)g.pitch, (cuuint64_t)g.Hp, (cuuint64_t)g.Dp, (cuuint64_t)(2 + K)};
+  const cuuint64_t str4[3] = {row, slab, (cuuint64_t)pb};
+  const cuuint32_t box4[4] = {32u, (cuuint32_t)ty, (cuuint32_t)tz, (cuuint32_t)(2 + K)};
+  const cuuint32_t unit[4] = {1u, 1u, 1u, 1u};
+  if (fn(&out[0], CU_TENSOR_MAP_DATA_TYPE_INT32, 4, g.e, dims4, str4, box4, unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
+         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  const cuuint32_t box3[3] = {40u, (cuuint32_t)(ty + 2), (cuuint32_t)(g.dims == 3 ? tz + 2 : 1)};
+  if (fn(&out[1], CU_TENSOR_MAP_DATA_TYPE_INT32, 3, g.h, dims4, str4, box3, unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
+         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  return true;
+}
+
 // Carve the control block for cap_tiles tiles / cap_grids grids.
 static void tileset_carve(TileSet& ts, char* blk, size_t* total) {
   const size_t nt = (size_t)ts.cap_tiles, ng = (size_t)ts.cap_grids;
@@ -113,6 +169,7 @@ static void tileset_carve(TileSet& ts, char* blk, size_t* total) {
   const size_t o_ctr = take(sizeof(DevCounters));
   const size_t o_ring = take(sizeof(unsigned long long) * nt * 2);   // work items: halves of split tiles
   const size_t o_lock = take(sizeof(int) * nt * 2);
+  const size_t o_tmap = take(kTmapBytes * ng);
   *total = off;
   if (!blk) return;
   ts.d_desc = (GridDev*)(blk + o_desc);
@@ -130,6 +187,7 @@ static void tileset_carve(TileSet& ts, char* blk, size_t* total) {
   ts.d_ctr = (DevCounters*)(blk + o_ctr);
   ts.d_pr_ring = (unsigned long long*)(blk + o_ring);
   ts.d_pr_lock = (int*)(blk + o_lock);
+  ts.tmap_slot = blk + o_tmap;
 }
 
 int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const std::vector<GridDev>& grids_in,
@@ -184,7 +242,9 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const st
   ts.ngrids = ngrids;
   ts.ntiles = ntiles;
   const size_t desc_bytes = sizeof(GridDev) * (size_t)ngrids, info_bytes = sizeof(int4) * (size_t)ntiles;
-  const size_t stage = align_up(desc_bytes, 256) + info_bytes;
+  const size_t tmap_bytes = kTmapBytes * (size_t)ngrids;
+  const size_t o_maps = align_up(align_up(desc_bytes, 256) + info_bytes, 256);
+  const size_t stage = o_maps + tmap_bytes;
   int4* info;
   if (s) {
     if (ts.h_stage_bytes < stage) {
@@ -201,6 +261,19 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const st
     v.resize(ntiles);
     info = v.data();
   }
+  // staging tensor maps (visits of the push-relabel shape: 32 x 8 halves of
+  // split 32 x 16 tiles)
+  static thread_local std::vector<CUtensorMap> mv;
+  CUtensorMap* maps;
+  if (s) {
+    maps = (CUtensorMap*)((char*)ts.h_stage + o_maps);
+  } else {
+    mv.resize(2 * (size_t)ngrids);
+    maps = mv.data();
+  }
+  bool tma = JFC_PR_TMA && ngrids > 0;
+  for (int gi = 0; gi < ngrids && tma; ++gi)
+    tma = encode_pr_maps(grids[gi], ts.pr_split ? 8 : TY, TZ, maps + 2 * gi);
   npar[0] = npar[1] = 0;
   size_t k = 0;
   for (size_t gi = 0; gi < grids.size(); ++gi) {
@@ -214,13 +287,16 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const st
   }
   ts.nlist[0] = npar[0];
   ts.nlist[1] = npar[1];
+  ts.d_tmap = tma ? ts.tmap_slot : nullptr;
   if (s) {
     // the staging buffer is rewritten only after the next host sync on `s`
     if (desc_bytes) JFC_CUDA(cudaMemcpyAsync(ts.d_desc, ts.h_stage, desc_bytes, cudaMemcpyHostToDevice, s));
     if (info_bytes) JFC_CUDA(cudaMemcpyAsync(ts.d_info, info, info_bytes, cudaMemcpyHostToDevice, s));
+    if (tma) JFC_CUDA(cudaMemcpyAsync((void*)ts.d_tmap, maps, tmap_bytes, cudaMemcpyHostToDevice, s));
   } else {
     if (desc_bytes) JFC_CUDA(cudaMemcpy(ts.d_desc, grids.data(), desc_bytes, cudaMemcpyHostToDevice));
     if (info_bytes) JFC_CUDA(cudaMemcpy(ts.d_info, info, info_bytes, cudaMemcpyHostToDevice));
+    if (tma) JFC_CUDA(cudaMemcpy((void*)ts.d_tmap, maps, tmap_bytes, cudaMemcpyHostToDevice));
   }
   return JFC_OK;
 }

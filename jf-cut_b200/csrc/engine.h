@@ -85,12 +85,12 @@ bool pr_split_for(const jfc_params& p, int dims);
 inline int interval_for(const jfc_params& p, int dims) {
   return p.relabel_interval > 0 ? p.relabel_interval : (dims == 2 ? 2 : 3);
 }
-// Distance cap of the global relabels while solving (0: none): relabel_cap,
-// or when it is 0 the measured default per dimensionality.  The Fast-Cut
-// comparison mode keeps the reference's exact relabels.
 // Push-relabel visit scheduling (1 sweeps, 2 worklist): pr_sched, or the
 // measured default when it is 0.
 inline int pr_sched_for(const jfc_params& p) { return p.pr_sched == 1 || p.pr_sched == 2 ? p.pr_sched : 1; }
+// Distance cap of the global relabels while solving (0: none): relabel_cap,
+// or when it is 0 the measured default per dimensionality.  The Fast-Cut
+// comparison mode keeps the reference's exact relabels.
 inline int relabel_cap_for(const jfc_params& p, int dims) {
   if (p.pr_mode == 1 || p.relabel_cap < 0) return 0;
   return p.relabel_cap > 0 ? p.relabel_cap : (dims == 2 ? 256 : 128);

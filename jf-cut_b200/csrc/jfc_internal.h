@@ -95,6 +95,11 @@ struct TileSet {
   int* d_grid_active = nullptr;      // [ngrids] active tiles after global relabel
   unsigned long long* d_pr_ring = nullptr;  // [work items] push-relabel worklist ring (null: sweeps only)
   int* d_pr_lock = nullptr;          // [work items] a visit of the item is in progress
+  const void* d_tmap = nullptr;      // [ngrids][2] tensor maps (128 B each) that stage push-relabel
+                                     // visits: the grid's planes {e, h, r...} with a tile box, and
+                                     // the h plane with a 40-wide tile + halo box (null: visits load
+                                     // their tiles with ordinary loads)
+  void* tmap_slot = nullptr;         // room for d_tmap in the control block
   long long* d_grid_sum = nullptr;   // [ngrids*2] sum min(e,0), source-side count
   DevCounters* d_ctr = nullptr;
   void* d_block = nullptr;           // single allocation backing the above
@@ -148,7 +153,8 @@ cudaError_t launch_set_limits(const TileSet& ts, unsigned long long polls, int h
 int persistent_blocks(const void* kernel, int threads, size_t smem);
 // persistent_blocks on the current device, cached per device in cache[64]
 // (every cooperative launch of one kernel reuses its grid size)
-int persistent_blocks_cached(int* cache, const void* kernel, int threads);
+// (smem: dynamic shared memory per block)
+int persistent_blocks_cached(int* cache, const void* kernel, int threads, size_t smem = 0);
 // layout helpers (kernels_bfs.cu)
 cudaError_t launch_fix_boundary(const GridDev& g, int conn, int* d_bad, cudaStream_t s);
 cudaError_t launch_pack_labels(const GridDev& g, uint8_t* d_dense, cudaStream_t s);

@@ -7,14 +7,17 @@
 namespace jfc {
 
 // One CTA per tile of 32 x TY (x TZ) nodes, one thread per node, one warp per
-// tile row.  Heights live in a shared-memory box with a one-cell halo.
-template <int DIMS, int TY_, int TZ_>
+// tile row.  Heights live in a shared-memory box with a one-cell halo; a row
+// of the box is HX_ wide and node x of the tile sits at column x + X0_ (the
+// push-relabel visit uses a 40-wide box starting 4 columns left of the tile,
+// the shape its tensor-copy staging lands in).
+template <int DIMS, int TY_, int TZ_, int HX_ = 34, int X0_ = 1>
 struct CtaTile {
-  static constexpr int TY = TY_, TZ = TZ_;
+  static constexpr int D = DIMS, TY = TY_, TZ = TZ_;
   static constexpr int R = TY * TZ;            // rows = warps
   static constexpr int NT = 32 * R;            // threads = nodes
   static constexpr int K = DIMS == 2 ? 4 : 6;  // arcs per node
-  static constexpr int HX = 34, HY = TY + 2, HZ = DIMS == 3 ? TZ + 2 : 1;
+  static constexpr int HX = HX_, X0 = X0_, HY = TY + 2, HZ = DIMS == 3 ? TZ + 2 : 1;
   static constexpr int HN = HX * HY * HZ;
   static constexpr int SY = HX, SZ = HX * HY; // box strides
   // arc slots (reference channel order)
@@ -25,7 +28,7 @@ struct CtaTile {
   static constexpr int NHY = 2 * TZ * 32, NHX = 2 * R, NHZ = DIMS == 3 ? 2 * TY * 32 : 0;
   static constexpr int NHALO = NHY + NHX + NHZ;
   __device__ static constexpr int hidx(int x, int y, int z) {
-    return ((DIMS == 3 ? (z + 1) * HY : 0) + (y + 1)) * HX + (x + 1);
+    return ((DIMS == 3 ? (z + 1) * HY : 0) + (y + 1)) * HX + (x + X0);
   }
   // halo cell c -> (x, y, z) relative to the tile origin and its face
   // (0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+)
@@ -95,9 +98,10 @@ __device__ __forceinline__ bool line_scan(int* h, int i, int stride, unsigned a,
 // step.  Monotone: reading a value another line just lowered is also valid.
 // `arc` holds each node's arc bits (tile order).  All threads of the CTA call
 // it; returns true when the fixpoint was reached within max_iter iterations.
-template <int DIMS, int TY, int TZ>
-__device__ bool relax_cta(int* h, const uint8_t* arc, int max_iter) {
-  using T = CtaTile<DIMS, TY, TZ>;
+// T: the tile geometry (CtaTile) the height box `h` is laid out in.
+template <class T>
+__device__ bool relax_cta_t(int* h, const uint8_t* arc, int max_iter) {
+  constexpr int DIMS = T::D, TY = T::TY, TZ = T::TZ;
   const int t = threadIdx.x;
   for (int it = 0; it < max_iter; ++it) {
     bool ch = false;
@@ -120,6 +124,11 @@ __device__ bool relax_cta(int* h, const uint8_t* arc, int max_iter) {
     if (!__syncthreads_or(ch)) return true;
   }
   return false;
+}
+
+template <int DIMS, int TY, int TZ>
+__device__ bool relax_cta(int* h, const uint8_t* arc, int max_iter) {
+  return relax_cta_t<CtaTile<DIMS, TY, TZ>>(h, arc, max_iter);
 }
 
 }  // namespace jfc

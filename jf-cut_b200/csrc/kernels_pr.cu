@@ -29,6 +29,7 @@
 // Heights only grow between global relabels (relabel = 1 + min over residual
 // arcs, applied to active nodes without an admissible arc).
 #include "jfc_relax.cuh"
+#include "jfc_tma.cuh"
 
 
 // Iteration cap of the exact local relabel at the start of a visit (0: none).
@@ -43,15 +44,32 @@ using jfc::FULL;
 template <int DIMS, int TY, int TZ>
 using Tile = jfc::CtaTile<DIMS, TY, TZ>;
 
+// Geometry of a visit's height box: 40 columns, node x at column x + 4 (the
+// box the tensor copy of the halo lands in: x0 - 4 .. x0 + 35 keeps its
+// first column on a 16-byte boundary).
+template <int DIMS, int TY, int TZ>
+using PrTile = jfc::CtaTile<DIMS, TY, TZ, 40, 4>;
+
+// Staging buffer of one visit, the working copy of the tile during it:
+// the tile's planes {e, h, r[0..K-1]} (plane-major, thread order) and the h
+// plane over the tile plus its one-cell halo.  The visit pushes and relabels
+// in place here.
+template <int DIMS, int TY, int TZ>
+struct alignas(128) PrStage {
+  using T = PrTile<DIMS, TY, TZ>;
+  static constexpr int P = 2 + T::K;
+  static constexpr unsigned kBytes = (unsigned)(sizeof(int) * (P * T::NT + T::HN));   // bytes one fill copies
+  int pl[P][T::NT];
+  int hb[T::HN];
+};
+
 template <int DIMS, int TY, int TZ>
 struct PrSmem {
-  using T = Tile<DIMS, TY, TZ>;
-  int e[T::NT];
-  int h[T::HN];
-  int r[T::K][T::NT];
+  using T = PrTile<DIMS, TY, TZ>;
   int out[T::NHALO];      // flow pushed into each halo cell during the visit
   uint8_t arc[T::NT];     // residual-arc bits for the local relabel
   int tile;
+  int buf;                // staging buffer of the item being visited
   int gen;                // worklist: generation of the item being visited
   int face[6];            // any flow left through face: x-, x+, y-, y+, z-, z+
   int q_nb[6];            // after a visit: the work item behind each face that received flow, or -1
@@ -86,43 +104,75 @@ __device__ __forceinline__ int face_item(const TileSet& ts, int tid, int f) {
   }
 }
 
-// One visit of work item `tid`; on return s.active tells whether the item still
-// holds an active node and s.q_nb[f] the item behind each face f that
-// received flow (-1: none).  The caller queues them.
+// Tile origin of work item `tid` (elements) and its grid.
 template <int DIMS, int TY, int TZ, bool SPLIT>
-__device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_iters, bool local_relabel,
-                                        PrSmem<DIMS, TY, TZ>& s) {
-  using T = Tile<DIMS, TY, TZ>;
-  const int t = threadIdx.x;
-  const int x = t & 31, row = t >> 5, y = row % TY, z = row / TY;
+__device__ __forceinline__ int4 item_origin(const TileSet& ts, int tid) {
   const int tile = SPLIT ? tid >> 1 : tid, half = SPLIT ? tid & 1 : 0;
   const int4 ti = ts.d_info[tile];
-  const GridDev& g = ts.d_desc[ti.x];
+  return make_int4(ti.x, ti.y * 32, SPLIT ? (2 * ti.z + half) * TY : ti.z * TY, ti.w * TZ);
+}
+
+// Fill staging buffer `st` with work item `tid` by two tensor copies (the
+// tile's planes, and the h plane over the tile and its halo), completed on
+// `bar`.  Issued by one thread.  Box cells outside the grid arrive as zeros;
+// the visit sets the halo ones to INF.
+template <int DIMS, int TY, int TZ, bool SPLIT>
+__device__ __forceinline__ void pr_stage_issue(const TileSet& ts, int tid, PrStage<DIMS, TY, TZ>& st, uint64_t* bar,
+                                               int& acquired_grid) {
+  const int4 o = item_origin<DIMS, TY, TZ, SPLIT>(ts, tid);
+  const char* maps = (const char*)ts.d_tmap + (size_t)o.x * 256;
+  if (o.x != acquired_grid) {
+    jfc::fence_tmap_acquire(maps);
+    jfc::fence_tmap_acquire(maps + 128);
+    acquired_grid = o.x;
+  }
+  jfc::fence_async_shared();   // the buffer's previous visit wrote it through the generic proxy
+  jfc::mbar_arrive_tx(bar, PrStage<DIMS, TY, TZ>::kBytes);
+  jfc::tma_load_4d(&st.pl[0][0], maps, o.y, o.z, o.w, 0, bar);
+  jfc::tma_load_3d(&st.hb[0], maps + 128, o.y - 4, o.z - 1, DIMS == 3 ? o.w - 1 : 0, bar);
+}
+
+// One visit of work item `tid` on staging buffer `st`; staged: the tensor
+// copies already filled it, otherwise the visit loads the tile itself.  On
+// return s.active tells whether the item still holds an active node and
+// s.q_nb[f] the item behind each face f that received flow (-1: none).  The
+// caller queues them.
+template <int DIMS, int TY, int TZ, bool SPLIT>
+__device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_iters, bool local_relabel,
+                                        PrSmem<DIMS, TY, TZ>& s, PrStage<DIMS, TY, TZ>& st, bool staged) {
+  using T = PrTile<DIMS, TY, TZ>;
+  const int t = threadIdx.x;
+  const int x = t & 31, row = t >> 5, y = row % TY, z = row / TY;
+  const int4 o = item_origin<DIMS, TY, TZ, SPLIT>(ts, tid);
+  const GridDev& g = ts.d_desc[o.x];
   const int pitch = g.pitch;
   const long long slab = (long long)g.pitch * g.Hp;
-  const int x0 = ti.y * 32, y0 = SPLIT ? (2 * ti.z + half) * TY : ti.z * TY, z0 = ti.w * TZ;
+  const int x0 = o.y, y0 = o.z, z0 = o.w;
   const long long tbase = (long long)x0 + (long long)y0 * pitch + (long long)z0 * slab;
   const long long n = tbase + x + (long long)y * pitch + (long long)z * slab;
   const int hi = T::hidx(x, y, z);
+  int* const se = st.pl[0];
+  int* const sh = st.hb;
   JFC_PCLK_DECL
 
-  // ---- stage the tile and its halo heights
-  const int e0 = g.e[n], h0 = g.h[n];
+  // ---- the tile and its halo heights
+  if (!staged) {
+    st.pl[0][t] = g.e[n];
+    st.pl[1][t] = g.h[n];
+#pragma unroll
+    for (int k = 0; k < T::K; ++k) st.pl[2 + k][t] = g.r[k][n];
+  }
+  const int e0 = st.pl[0][t], h0 = st.pl[1][t];
   int r0[T::K];
 #pragma unroll
-  for (int k = 0; k < T::K; ++k) r0[k] = g.r[k][n];
-  s.e[t] = e0;
-  s.h[hi] = h0;
-#pragma unroll
-  for (int k = 0; k < T::K; ++k) s.r[k][t] = r0[k];
+  for (int k = 0; k < T::K; ++k) r0[k] = st.pl[2 + k][t];
   for (int c = t; c < T::NHALO; c += T::NT) {
     int hx, hy, hz, f;
     halo_cell<DIMS, TY, TZ>(c, hx, hy, hz, f);
     const int gx = x0 + hx, gy = y0 + hy, gz = z0 + hz;
-    int v = JFC_INF;
-    if (gx >= 0 && gx < pitch && gy >= 0 && gy < g.Hp && gz >= 0 && gz < g.Dp)
-      v = g.h[(long long)gx + (long long)gy * pitch + (long long)gz * slab];
-    s.h[T::hidx(hx, hy, hz)] = v;
+    const bool in = gx >= 0 && gx < pitch && gy >= 0 && gy < g.Hp && gz >= 0 && gz < g.Dp;
+    if (!staged || !in)
+      sh[T::hidx(hx, hy, hz)] = in ? g.h[(long long)gx + (long long)gy * pitch + (long long)gz * slab] : JFC_INF;
     s.out[c] = 0;
   }
   if (t < 6) s.face[t] = 0;
@@ -142,7 +192,7 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
     // The pointwise max of two valid labellings is valid, so heights stay
     // monotone (push-relabel termination holds) while excess trapped in the
     // tile jumps straight to INF instead of climbing one level per round.
-    s.h[hi] = e0 < 0 ? 0 : JFC_INF;
+    sh[hi] = e0 < 0 ? 0 : JFC_INF;
   }
   __syncthreads();
   JFC_PCLK(ts.d_ctr, 0);
@@ -152,13 +202,13 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
   if (JFC_LOCAL_RELABEL_ITERS > 0 && local_relabel) {
     // a partial relaxation overestimates distances, so the local labelling
     // is only applied when the in-tile fixpoint was reached
-    const bool exact = jfc::relax_cta<DIMS, TY, TZ>(s.h, s.arc, JFC_LOCAL_RELABEL_ITERS);
-    hown = exact ? max(s.h[hi], h0) : h0;
+    const bool exact = jfc::relax_cta_t<T>(sh, s.arc, JFC_LOCAL_RELABEL_ITERS);
+    hown = exact ? max(sh[hi], h0) : h0;
 #ifdef JFC_PHASE_CLOCK
     if (threadIdx.x == 0 && exact) atomicAdd(&ts.d_ctr->prof[5], 1ull);
 #endif
   }
-  s.h[hi] = hown;
+  sh[hi] = hown;
   __syncthreads();
   JFC_PCLK(ts.d_ctr, 1);
 
@@ -184,7 +234,7 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
     // changes them between the relabel step and the push step, and the
     // credits neighbours add during the push step only raise them, so these
     // values bound what the node may push from below
-    const int e = s.e[t];
+    const int e = se[t];
     const bool act = e > 0 && hown < JFC_INF;
     int rk[NP];
     // relabel every active node without an admissible arc, in place
@@ -195,8 +245,8 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
       int hn[NP];
 #pragma unroll
       for (int q = 0; q < NP; ++q) {
-        rk[q] = s.r[slot(q)][t];
-        hn[q] = s.h[hi + hoff(q)];
+        rk[q] = st.pl[2 + slot(q)][t];
+        hn[q] = sh[hi + hoff(q)];
       }
       const int hm = hown - 1;
       bool adm = false;
@@ -208,7 +258,7 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
       }
       if (!adm) {
         hown = max(hown, min(m + 1, JFC_INF));
-        s.h[hi] = hown;
+        sh[hi] = hown;
         did = true;
       }
     }
@@ -225,7 +275,7 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
         const int hcell[6] = {hc_xp, hc_yp, hc_ym, DIMS == 3 ? hc_zp : hc_xm, hc_zm, hc_xm};
         int hn[NP], d[NP];
 #pragma unroll
-        for (int q = 0; q < NP; ++q) hn[q] = s.h[hi + hoff(q)];
+        for (int q = 0; q < NP; ++q) hn[q] = sh[hi + hoff(q)];
         int ex = e;
 #pragma unroll
         for (int q = 0; q < NP; ++q) {
@@ -236,16 +286,16 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
 #pragma unroll
           for (int q = 0; q < NP; ++q) {
             if (d[q]) {
-              s.r[slot(q)][t] = rk[q] - d[q];
+              st.pl[2 + slot(q)][t] = rk[q] - d[q];
               if (inside[q == NP - 1 ? 5 : q]) {
-                atomicAdd(&s.e[t + toff(q)], d[q]);
-                atomicAdd(&s.r[T::K - 1 - slot(q)][t + toff(q)], d[q]);
+                atomicAdd(&se[t + toff(q)], d[q]);
+                atomicAdd(&st.pl[2 + T::K - 1 - slot(q)][t + toff(q)], d[q]);
               } else {
                 s.out[hcell[q == NP - 1 ? 5 : q]] += d[q];
               }
             }
           }
-          atomicAdd(&s.e[t], ex - e);
+          atomicAdd(&se[t], ex - e);
           did = true;
         }
       }
@@ -255,14 +305,22 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
   const int rounds = it < local_iters ? it + 1 : local_iters;
   JFC_PCLK(ts.d_ctr, 2);
 
-  // ---- write back the words that changed
-  const int e1 = s.e[t], h1 = hown;
-  if (e1 != e0) g.e[n] = e1;
-  if (h1 != h0) g.h[n] = h1;
+  // ---- write back: each row's 4-node groups holding a changed word, as
+  //      128-bit stores (nothing else writes the tile while it is visited, so
+  //      the unchanged words of a group are rewritten with their own values)
+  const int e1 = se[t], h1 = hown;
+  {
+    const long long nrow = n - x;
+    const int grp = x & ~3;
+    auto put = [&](int* gplane, const int* srow, bool changed) {
+      const unsigned m = __ballot_sync(jfc::FULL, changed);
+      if ((x & 3) == 0 && ((m >> grp) & 0xFu))
+        *reinterpret_cast<int4*>(gplane + nrow + grp) = *reinterpret_cast<const int4*>(srow + grp);
+    };
+    put(g.e, se + row * 32, e1 != e0);
+    put(g.h, sh + T::hidx(0, y, z), h1 != h0);
 #pragma unroll
-  for (int k = 0; k < T::K; ++k) {
-    const int v = s.r[k][t];
-    if (v != r0[k]) g.r[k][n] = v;
+    for (int k = 0; k < T::K; ++k) put(g.r[k], st.pl[2 + k] + row * 32, st.pl[2 + k][t] != r0[k]);
   }
   // ---- send the flow pushed across the border into the neighbours' excess
   //      and reverse arcs (only halo cells inside the grid can receive flow:
@@ -297,13 +355,36 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
 // by grid barriers.  Sweep s of parity p drains queue q_pr[p][cur_pr[p]] one
 // tile per CTA ticket; tiles still active go to q_pr[p][1-cur], neighbours
 // that received flow to the other parity's pending buffer.
+//
+// Staging (ts.d_tmap set): tensor copies fill one of two staging buffers in
+// dynamic shared memory.  While a visit runs, the CTA's next ticket is
+// already being copied into the other buffer, as long as the sweep holds at
+// least a grid's worth of tickets beyond the current one (in a short sweep
+// a second ticket would only keep another CTA idle).  A prefetched item is
+// safe to read early: items of one sweep are never adjacent, so nothing
+// writes its tile or its halo heights until the sweep ends.
 template <int DIMS, int TY, int TZ, bool SPLIT>
 __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
     k_pr_phase(TileSet ts, int sweeps, int local_iters) {
+  using Stage = PrStage<DIMS, TY, TZ>;
   __shared__ PrSmem<DIMS, TY, TZ> sm;
+  __shared__ uint64_t s_bar[2];
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  Stage* stage = reinterpret_cast<Stage*>(s_dyn + ((128u - (jfc::smem_addr(s_dyn) & 127u)) & 127u));
   DevCounters* ctr = ts.d_ctr;
+  const bool tma = ts.d_tmap != nullptr;
   unsigned long long visits = 0, rounds = 0;
   const unsigned long long t0 = jfc::global_ns();
+  const unsigned long long cap = jfc::spin_cap(ctr);
+  if (tma && threadIdx.x == 0) {
+    jfc::mbar_init(&s_bar[0], 1);
+    jfc::mbar_init(&s_bar[1], 1);
+    jfc::fence_mbar_init();
+  }
+  __syncthreads();
+  unsigned parity = 0;      // bit b: phase parity of buffer b's next fill
+  int acquired_grid = -1;   // thread 0: grid whose tensor maps it acquired
+  int next_buf = 0;         // thread 0: buffer of the next fill
   int s = 0;
   const int npairs = sweeps > 0 ? sweeps : jfc::vload(&ctr->pr_sweeps);
   for (; s < 2 * npairs; ++s) {
@@ -313,19 +394,63 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
     const int n = jfc::vload(&ctr->qn_pr[p][b]);
     if (n == 0 && jfc::vload(&ctr->qn_pr[p ^ 1][bo]) == 0) break;  // nothing left anywhere
     const int* queue = ts.d_q_pr[p][b];
+    // the previous sweep's writes (seen through the grid barrier) come before
+    // this sweep's tensor reads
+    if (tma && threadIdx.x == 0) jfc::fence_async_global();
+    int pre = -1, pre_buf = 0;   // thread 0: the prefetched item and its buffer
+    unsigned pre_k = 0;
+    bool failed = false;
     for (;;) {
       if (threadIdx.x == 0) {
-        const unsigned k = atomicAdd(&ctr->ticket[s & 1], 1u);
-        sm.tile = (int)k < n ? queue[k] : -1;
-        if ((int)k < n) ts.d_flag_pr[sm.tile] = 0;
+        int item, buf = 0;
+        unsigned k;
+        if (pre >= 0) {
+          item = pre; buf = pre_buf; k = pre_k; pre = -1;
+        } else {
+          k = atomicAdd(&ctr->ticket[s & 1], 1u);
+          item = (int)k < n ? queue[k] : -1;
+          if (item >= 0) {
+            ts.d_flag_pr[item] = 0;
+            if (tma) {
+              buf = next_buf; next_buf ^= 1;
+              pr_stage_issue<DIMS, TY, TZ, SPLIT>(ts, item, stage[buf], &s_bar[buf], acquired_grid);
+            }
+          }
+        }
+        if (tma && item >= 0 && (long long)k + gridDim.x < n) {
+          const unsigned k2 = atomicAdd(&ctr->ticket[s & 1], 1u);
+          if ((int)k2 < n) {
+            pre = queue[k2];
+            pre_k = k2;
+            ts.d_flag_pr[pre] = 0;
+            pre_buf = next_buf; next_buf ^= 1;
+            pr_stage_issue<DIMS, TY, TZ, SPLIT>(ts, pre, stage[pre_buf], &s_bar[pre_buf], acquired_grid);
+          }
+        }
+        sm.tile = item;
+        sm.buf = buf;
       }
       __syncthreads();
-      const int tid = sm.tile;
+      const int tid = sm.tile, buf = sm.buf;
       if (tid < 0) break;
+      if (tma) {
+        const bool ok = jfc::mbar_wait(&s_bar[buf], (parity >> buf) & 1u, cap);
+        parity ^= 1u << buf;
+        if (__syncthreads_or(!ok)) {
+          if (threadIdx.x == 0) {
+            atomicExch(&ctr->error, 1);
+            // copies still in flight land before the CTA leaves (bounded)
+            jfc::mbar_wait(&s_bar[buf], ((parity >> buf) & 1u) ^ 1u, cap);
+            if (pre >= 0) jfc::mbar_wait(&s_bar[pre_buf], (parity >> pre_buf) & 1u, cap);
+          }
+          failed = true;
+          break;
+        }
+      }
       // first sweep of a phase: nothing moved since the exact global relabel
       // (the halo tiles have the other parity), so the local relabel would
       // reproduce the heights it finds
-      rounds += pr_visit<DIMS, TY, TZ, SPLIT>(ts, tid, local_iters, s > 0, sm);
+      rounds += pr_visit<DIMS, TY, TZ, SPLIT>(ts, tid, local_iters, s > 0, sm, stage[buf], tma);
       ++visits;
       // queue: myself for my parity's next sweep, neighbours for the other parity
       if (threadIdx.x < 32) {
@@ -338,6 +463,7 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
       }
       __syncthreads();
     }
+    if (failed) break;   // a staging copy never completed (error raised): leave
     JFC_PCLK_DECL
     const bool ok = jfc::grid_sync(ctr, [&]() {
       ctr->ticket[s & 1] = 0;
@@ -402,6 +528,9 @@ template <int DIMS, int TY, int TZ, bool SPLIT>
 __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
     k_pr_async(TileSet ts, int sweeps, int local_iters) {
   __shared__ PrSmem<DIMS, TY, TZ> sm;
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  PrStage<DIMS, TY, TZ>& stage =
+      *reinterpret_cast<PrStage<DIMS, TY, TZ>*>(s_dyn + ((128u - (jfc::smem_addr(s_dyn) & 127u)) & 127u));
   DevCounters* ctr = ts.d_ctr;
   const unsigned long long t0 = jfc::global_ns();
   const int npairs = sweeps > 0 ? sweeps : jfc::vload(&ctr->pr_sweeps);
@@ -495,7 +624,7 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
     // generation 0: nothing around the item moved since the exact global
     // relabel unless a neighbour was visited first; the local relabel is an
     // improvement only, so skipping it is safe either way
-    rounds += pr_visit<DIMS, TY, TZ, SPLIT>(ts, item, local_iters, gen > 0, sm);
+    rounds += pr_visit<DIMS, TY, TZ, SPLIT>(ts, item, local_iters, gen > 0, sm, stage, false);
     ++visits;
     maxgen = max(maxgen, gen);
     // release the item (its writes visible first), then queue what it fed
@@ -545,12 +674,19 @@ cudaError_t launch_t(const TileSet& ts, int sweeps, int local_iters, cudaStream_
   constexpr int NT = Tile<DIMS, TY, TZ>::NT;
   const bool async = sched == 2 && ts.d_pr_ring != nullptr;
   const void* fn = async ? (const void*)k_pr_async<DIMS, TY, TZ, SPLIT> : (const void*)k_pr_phase<DIMS, TY, TZ, SPLIT>;
+  // staging buffers in dynamic shared memory: two for the sweeps (one being
+  // visited, one being filled), one for the worklist; + 128 B to align them
+  const size_t dyn = sizeof(PrStage<DIMS, TY, TZ>) * (async ? 1 : 2) + 128;
   static int cache_sweeps[64] = {0}, cache_async[64] = {0};
-  const int blocks = persistent_blocks_cached(async ? cache_async : cache_sweeps, fn, NT);
+  if (dyn > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e != cudaSuccess) return e;
+  }
+  const int blocks = persistent_blocks_cached(async ? cache_async : cache_sweeps, fn, NT, dyn);
   TileSet arg = ts;
   void* params[] = {(void*)&arg, (void*)&sweeps, (void*)&local_iters};
   jfc_note_launch();
-  return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(NT), params, 0, st);
+  return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(NT), params, dyn, st);
 }
 
 // Local pre-push before the first relabel of a solve, one CTA per tile, the

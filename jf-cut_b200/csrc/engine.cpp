@@ -532,12 +532,16 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   auto total = [&]() { long long t = 0; for (int v : active) t += v; return t; };
   const DevCounters* hc = (const DevCounters*)ctx->h_pin;
   double prev_pr = 0.0, prev_gr = 0.0, prev_grf = 0.0;
+  unsigned long long prev_vis = 0;
   if (p.verbose) {   // the first relabel's share
     const DevCounters* c0 = (const DevCounters*)ctx->h_pin;
     prev_gr = (c0->ns_gr_first + c0->ns_gr_frontier) * 1e-6;
     prev_grf = c0->ns_gr_first * 1e-6;
-    fprintf(stderr, "{\"relabel\": 1, \"active_tiles\": %lld, \"ms_gr\": %.3f, \"ms_gr_dense\": %.3f}\n",
-            [&]() { long long t = 0; for (int v : active) t += v; return t; }(), prev_gr, prev_grf);
+    prev_vis = c0->bfs_visits;
+    fprintf(stderr, "{\"relabel\": 1, \"active_tiles\": %lld, \"ms_gr\": %.3f, \"ms_gr_dense\": %.3f, "
+                    "\"gr_passes\": %d, \"gr_visits\": %llu}\n",
+            [&]() { long long t = 0; for (int v : active) t += v; return t; }(), prev_gr, prev_grf, c0->bfs_passes,
+            c0->bfs_visits);
   }
   int status = JFC_OK;
   // Adaptive schedule: while a large part of the grid is active, frequent
@@ -608,8 +612,10 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
       const double pr = hc->ns_pr * 1e-6, gr = (hc->ns_gr_first + hc->ns_gr_frontier) * 1e-6;
       const double grf = hc->ns_gr_first * 1e-6;
       fprintf(stderr, "{\"relabel\": %d, \"sweeps\": %d, \"active_tiles\": %lld, \"ms_pr\": %.3f, \"ms_gr\": %.3f, "
-                      "\"ms_gr_dense\": %.3f}\n",
-              st.global_relabels, st.sweeps, total(), pr - prev_pr, gr - prev_gr, grf - prev_grf);
+                      "\"ms_gr_dense\": %.3f, \"gr_passes\": %d, \"gr_visits\": %llu}\n",
+              st.global_relabels, st.sweeps, total(), pr - prev_pr, gr - prev_gr, grf - prev_grf, hc->bfs_passes,
+              hc->bfs_visits - prev_vis);
+      prev_vis = hc->bfs_visits;
       prev_pr = pr;
       prev_gr = gr;
       prev_grf = grf;

@@ -850,6 +850,173 @@ __device__ __forceinline__ void relabel_frontier_warp(const TileSet& ts, int tid
   flag_neighbours<DIMS, TY, TZ>(g, a, tid, rows_changed, c0 != 0, c31 != 0, again, Q);
 }
 
+// x-direction closure of one tile row (lane = x): h(p) = min(h(p), h(q) + |p - q|)
+// over the runs of residual arcs p -> p+1 -> ... -> q (axp) and p -> p-1 ->
+// ... -> q (axm), by doubling.  The arc runs are read from the row's arc
+// masks, so only the values move between lanes.
+__device__ __forceinline__ int row_close(int v, unsigned axp, unsigned axm, int lane) {
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int nv = __shfl_down_sync(FULL, v, off);
+    const unsigned run = (1u << off) - 1u;
+    if (lane + off < 32 && ((~axp >> lane) & run) == 0u) v = min(v, nv + off);
+  }
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int nv = __shfl_up_sync(FULL, v, off);
+    const unsigned run = (1u << off) - 1u;
+    if (lane >= off && ((~axm >> (lane - off + 1)) & run) == 0u) v = min(v, nv + off);
+  }
+  return v;
+}
+
+// Frontier visit, one warp per tile, min-plus form: the tile's heights in
+// registers (lane = x, one register per row), lowered by the halo heights
+// across residual arcs, then closed in place: row closures by doubling
+// shuffles, y and z runs in registers (a forward and a backward sweep per
+// line), repeated until nothing falls.  Monotone, so the fixpoint is the
+// exact in-tile distance given the halo, as the level BFS gives; a visit
+// costs one closure per turn a shortest path takes instead of one step per
+// level.  Improvements at or above the distance cap are dropped (those
+// nodes stay unreachable).
+template <int DIMS, int TY, int TZ>
+__device__ __forceinline__ void relabel_frontier_minplus(const TileSet& ts, int tid, const BfsQ& Q, int& cur_grid,
+                                                         int& delta) {
+  constexpr int R = TY * TZ;
+  const int lane = threadIdx.x & 31;
+  const int4 ti = ts.d_info[tid];
+  const GridDev& g = ts.d_desc[ti.x];
+  const Addr a = make_addr<DIMS, TY, TZ>(g, ti, lane);
+  unsigned lab[R];
+  int hv[R], h0[R];
+  unsigned AXP[R], AXM[R];
+  unsigned posm = 0;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const long long n = roff<TY>(a, i);
+    lab[i] = g.label[n];   // arc byte written by the first pass
+    h0[i] = g.h[n];
+  }
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    hv[i] = h0[i];
+    AXP[i] = __ballot_sync(FULL, lab[i] & jfc::A_XP);
+    AXM[i] = __ballot_sync(FULL, lab[i] & jfc::A_XM);
+    if (lab[i] & 128u) posm |= 1u << i;
+  }
+  // the halo, fixed during the visit: y faces per z slice (lane = x), z
+  // faces per row y, x faces in lanes r (left of row r) and 16 + r (right)
+#pragma unroll
+  for (int z = 0; z < TZ; ++z) {
+    const int it = z * TY, ib = z * TY + TY - 1;
+    const long long n = roff<TY>(a, it);
+    if (a.has_yT && (lab[it] & jfc::A_YM)) hv[it] = min(hv[it], g.h[n - a.pitch] + 1);
+    if (a.has_yB && (lab[ib] & jfc::A_YP)) hv[ib] = min(hv[ib], g.h[n + (long long)TY * a.pitch] + 1);
+  }
+  if constexpr (DIMS == 3) {
+#pragma unroll
+    for (int y = 0; y < TY; ++y) {
+      const int it = y, ib = (TZ - 1) * TY + y;
+      const long long n = roff<TY>(a, y);
+      if (a.has_zT && (lab[it] & jfc::A_ZM)) hv[it] = min(hv[it], g.h[n - a.slab] + 1);
+      if (a.has_zB && (lab[ib] & jfc::A_ZP)) hv[ib] = min(hv[ib], g.h[n + (long long)TZ * a.slab] + 1);
+    }
+  }
+  {
+    const int xrow = lane & 15;
+    const bool left = lane < 16;
+    int hx = JFC_INF;
+    if (xrow < R && (left ? a.has_xL : a.has_xR))
+      hx = g.h[(long long)(left ? a.x0 - 1 : a.x0 + 32) + (long long)(a.y0 + xrow % TY) * a.pitch +
+               (long long)(a.z0 + xrow / TY) * a.slab];
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int hl = __shfl_sync(FULL, hx, i), hr = __shfl_sync(FULL, hx, 16 + i);
+      if (lane == 0 && (lab[i] & jfc::A_XM)) hv[i] = min(hv[i], hl + 1);
+      if (lane == 31 && (lab[i] & jfc::A_XP)) hv[i] = min(hv[i], hr + 1);
+    }
+  }
+  // closure to the fixpoint (bounded by the tile's nodes: every pass but the
+  // last lowers some height, and heights are bounded below by 0)
+  for (int pass = 0; pass < 32 * R; ++pass) {
+    bool ch = false;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int v = row_close(hv[i], AXP[i], AXM[i], lane);
+      ch |= v < hv[i];
+      hv[i] = v;
+    }
+#pragma unroll
+    for (int z = 0; z < TZ; ++z) {
+#pragma unroll
+      for (int y = TY - 2; y >= 0; --y) {
+        const int i = z * TY + y;
+        if ((lab[i] & jfc::A_YP) && hv[i + 1] + 1 < hv[i]) { hv[i] = hv[i + 1] + 1; ch = true; }
+      }
+#pragma unroll
+      for (int y = 1; y < TY; ++y) {
+        const int i = z * TY + y;
+        if ((lab[i] & jfc::A_YM) && hv[i - 1] + 1 < hv[i]) { hv[i] = hv[i - 1] + 1; ch = true; }
+      }
+    }
+    if constexpr (DIMS == 3) {
+#pragma unroll
+      for (int y = 0; y < TY; ++y) {
+#pragma unroll
+        for (int z = TZ - 2; z >= 0; --z) {
+          const int i = z * TY + y;
+          if ((lab[i] & jfc::A_ZP) && hv[i + TY] + 1 < hv[i]) { hv[i] = hv[i + TY] + 1; ch = true; }
+        }
+#pragma unroll
+        for (int z = 1; z < TZ; ++z) {
+          const int i = z * TY + y;
+          if ((lab[i] & jfc::A_ZM) && hv[i - TY] + 1 < hv[i]) { hv[i] = hv[i - TY] + 1; ch = true; }
+        }
+      }
+    }
+    if (!__any_sync(FULL, ch)) break;
+  }
+  const int cap = jfc::cap_of(g, ts.d_ctr);
+  unsigned rows_changed = 0;
+  bool c0 = false, c31 = false, act_lo = false, act_hi = false;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    if (hv[i] >= cap) hv[i] = h0[i];   // at or above the cap: stays as it was (unreachable)
+    const bool chg = hv[i] < h0[i];
+    const unsigned m = __ballot_sync(FULL, chg);
+    if (m) {
+      rows_changed |= 1u << i;
+      c0 |= (m & 1u) != 0;
+      c31 |= (m >> 31) != 0;
+    }
+    if (chg) g.h[roff<TY>(a, i)] = hv[i];
+    // activity per 8-row half of a 2D 32x16 tile (bit 0 rows 0-7, bit 1
+    // rows 8-15: the push-relabel work items of split tile sets), else bit 0
+    const bool live = ((posm >> i) & 1u) && hv[i] < JFC_INF;
+    if (DIMS == 2 && TY == 16 && i >= 8) act_hi |= live;
+    else act_lo |= live;
+  }
+  act_lo = __any_sync(FULL, act_lo);
+  act_hi = __any_sync(FULL, act_hi);
+  const bool act = act_lo || act_hi;
+  if (lane == 0) {
+    const int old = (ts.d_act[tid] & 3u) != 0 ? 1 : 0;
+    ts.d_act[tid] = (uint8_t)((act_lo ? 1 : 0) | (act_hi ? 2 : 0));
+    if (ti.x != cur_grid) {
+      if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
+      delta = 0;
+      cur_grid = ti.x;
+    }
+    delta += (act ? 1 : 0) - old;
+  }
+  flag_neighbours<DIMS, TY, TZ>(g, a, tid, rows_changed, c0, c31, false, Q);
+}
+
+// 1: frontier visits of the warp form use the min-plus closure, 0: the level BFS
+#ifndef JFC_RELABEL_MINPLUS
+#define JFC_RELABEL_MINPLUS 1
+#endif
+
 #ifndef JFC_GR_ASYNC
 #define JFC_GR_ASYNC 1
 #endif
@@ -916,11 +1083,14 @@ __global__ void __launch_bounds__(256, (DIMS == 3 && TY * TZ > 8) ? 1 : (DIMS ==
 // graphcut_count_block.cl:19-65, as one warp-aggregated append).
 // Warp form of the frontier passes: one warp per queued tile (3D: many
 // tiles per pass, so the visit throughput counts).
-template <int DIMS, int TY, int TZ>
+// (level-BFS form: one CTA per SM, its registers; min-plus form: 3 CTAs per
+// SM for 8-row tiles, 2 for 16-row ones, without spills)
 #ifndef JFC_RELABEL_WARP_MINB
 #define JFC_RELABEL_WARP_MINB 1
 #endif
-__global__ void __launch_bounds__(256, JFC_RELABEL_WARP_MINB) k_relabel_warp(TileSet ts, int max_passes) {
+template <int DIMS, int TY, int TZ>
+__global__ void __launch_bounds__(256, JFC_RELABEL_MINPLUS ? (TY * TZ > 8 ? 2 : 3) : JFC_RELABEL_WARP_MINB)
+    k_relabel_warp(TileSet ts, int max_passes) {
   DevCounters* ctr = ts.d_ctr;
   const int lane = threadIdx.x & 31;
   unsigned long long visits = 0;
@@ -945,7 +1115,8 @@ __global__ void __launch_bounds__(256, JFC_RELABEL_WARP_MINB) k_relabel_warp(Til
       const int tt = queue[k];
       if (lane == 0) fcur[tt] = 0;
       __syncwarp();
-      relabel_frontier_warp<DIMS, TY, TZ>(ts, tt, Q, cur_grid, delta);
+      if (JFC_RELABEL_MINPLUS) relabel_frontier_minplus<DIMS, TY, TZ>(ts, tt, Q, cur_grid, delta);
+      else relabel_frontier_warp<DIMS, TY, TZ>(ts, tt, Q, cur_grid, delta);
       ++visits;
     }
     ok = jfc::grid_sync(ctr, [&]() {
@@ -1347,15 +1518,15 @@ int persistent_blocks(const void* kernel, int threads, size_t smem) {
   return sms * per;
 }
 
-int persistent_blocks_cached(int* cache, const void* kernel, int threads) {
+int persistent_blocks_cached(int* cache, const void* kernel, int threads, size_t smem) {
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64) return persistent_blocks(kernel, threads, 0);
+  if (dev < 0 || dev >= 64) return persistent_blocks(kernel, threads, smem);
   // two threads filling one entry at once compute the same value; the
   // atomic store keeps the write whole
   int v = __atomic_load_n(cache + dev, __ATOMIC_RELAXED);
   if (!v) {
-    v = persistent_blocks(kernel, threads, 0);
+    v = persistent_blocks(kernel, threads, smem);
     __atomic_store_n(cache + dev, v, __ATOMIC_RELAXED);
   }
   return v;

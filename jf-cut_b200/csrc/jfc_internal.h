@@ -70,8 +70,9 @@ struct DevCounters {
   unsigned pr_tail;          // push-relabel worklist: ring positions reserved
   int pr_out;                // push-relabel worklist: items queued and not yet fully visited
   unsigned wl_head;          // 2D relabel worklist: tickets taken
-  unsigned wl_tail;          // 2D relabel worklist: ring positions reserved
-  int wl_out;                // 2D relabel worklist: items queued and not yet fully visited
+  unsigned long long wl_tail_out;  // 2D relabel worklist, updated together: ring positions
+                                   // reserved (high 32 bits) and items queued and not yet fully
+                                   // visited (low 32 bits)
 };
 
 // A set of grids tiled with one tile shape: the unit every launch works on

@@ -37,7 +37,25 @@ struct BfsQ {
   int* flags;
   int* q;
   int* qn;
+  // staging in shared memory (null: appends go straight to the queue): the
+  // items that won their flag are collected in sbuf (count *scnt) and the
+  // caller moves them to the queue with one counter update per batch, so
+  // thousands of warps do not all serialise on the queue's one counter
+  // (the warp form of the 3D frontier passes)
+  int* sbuf = nullptr;
+  int* scnt = nullptr;
 };
+
+// Move a warp's staged items of Q to its queue with one counter update (all
+// lanes, after a __syncwarp; the caller resets the count).
+__device__ __forceinline__ void flush_staged(const BfsQ& Q, int lane) {
+  const int cnt = *(volatile int*)Q.scnt;
+  if (cnt == 0) return;
+  int base = 0;
+  if (lane == 0) base = atomicAdd(Q.qn, cnt);
+  base = __shfl_sync(FULL, base, 0);
+  for (int i = lane; i < cnt; i += 32) Q.q[base + i] = Q.sbuf[i];
+}
 
 // Worklist of the asynchronous 2D relabel: a ring of `cap` tile slots (-1 =
 // empty) with the queued flags of BfsQ, a tail counter and the count of
@@ -45,8 +63,7 @@ struct BfsQ {
 struct RlRing {
   int* ring;
   unsigned cap;
-  unsigned* tail;
-  int* out;
+  unsigned long long* tail_out;   // ring positions reserved (high 32 bits), items outstanding (low 32)
   int* err;
   unsigned long long max_spins;   // polls before a wait gives up
 };
@@ -56,16 +73,21 @@ struct RlRing {
 // while one is on its way), then reserve ring positions and claim each slot
 // (free, or freed by its reader within a few polls; bounded: after
 // W.max_spins polls the error flag is raised).  Returns false after an error.
-__device__ __forceinline__ bool ring_append(bool want, int tile, int* flags, const RlRing& W) {
+// Returns false after an error.  `folded` tells whether the appending visit's
+// own completion was counted in the same update (it appended something): the
+// update adds m positions and m - 1 outstanding items, made before the items
+// are published, so the count cannot reach zero while they wait.
+__device__ __forceinline__ bool ring_append(bool want, int tile, int* flags, const RlRing& W, bool& folded) {
   bool won = false;
   if (want) won = atomicExch(flags + tile, 1) == 0;
   const unsigned m = __ballot_sync(jfc::FULL, won);
+  folded = m != 0;
   if (!m) return true;
   const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
   unsigned base = 0;
   if (lane == leader) {
-    atomicAdd(W.out, __popc(m));
-    base = atomicAdd(W.tail, (unsigned)__popc(m));
+    const unsigned c = (unsigned)__popc(m);
+    base = (unsigned)(atomicAdd(W.tail_out, ((unsigned long long)c << 32) + (c - 1u)) >> 32);
   }
   base = __shfl_sync(jfc::FULL, base, leader);
   bool ok = true;
@@ -142,7 +164,11 @@ __device__ __forceinline__ void flag_neighbours(const GridDev& g, const Addr& a,
     case 6: want = again; nb = tid; break;
     default: break;
   }
-  jfc::warp_append(want, nb, Q.flags, Q.q, Q.qn);
+  if (Q.sbuf) {
+    if (want && atomicExch(Q.flags + nb, 1) == 0) Q.sbuf[atomicAdd(Q.scnt, 1)] = nb;
+  } else {
+    jfc::warp_append(want, nb, Q.flags, Q.q, Q.qn);
+  }
 }
 
 // ------------------------------------------------------------------ cut BFS
@@ -430,6 +456,7 @@ struct RlSmem {
   uint8_t arc[RTile<DIMS, TY, TZ>::NT];
   int ntile;
   int face[6];
+  int folded;   // worklist: the visit's completion was counted with its appends
 };
 
 // One frontier visit, one CTA per tile, one thread per node (the reference's
@@ -441,7 +468,7 @@ struct RlSmem {
 template <int DIMS, int TY, int TZ>
 __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem<DIMS, TY, TZ>& s,
                                               const BfsQ& Q, int& cur_grid, int& delta,
-                                              const RlRing& W = RlRing{nullptr, 0, nullptr, nullptr, nullptr}) {
+                                              const RlRing& W = RlRing{nullptr, 0, nullptr, nullptr, 0}) {
   using T = RTile<DIMS, TY, TZ>;
   using D = Dirs<DIMS>;
   const int t = threadIdx.x;
@@ -531,8 +558,13 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
       case 6: want = !converged; nb = tid; break;
       default: break;
     }
-    if (W.ring) ring_append(want, nb, Q.flags, W);
-    else jfc::warp_append(want, nb, Q.flags, Q.q, Q.qn);
+    if (W.ring) {
+      bool folded = false;
+      ring_append(want, nb, Q.flags, W, folded);
+      if (t == 0) s.folded = folded ? 1 : 0;
+    } else {
+      jfc::warp_append(want, nb, Q.flags, Q.q, Q.qn);
+    }
     if (t == 0) {
       const int old = ((fresh ? __ldcg(ts.d_act + tid) : ts.d_act[tid]) & 3u) != 0 ? 1 : 0;
       ts.d_act[tid] = (uint8_t)((act_lo ? 1 : 0) | (act_hi ? 2 : 0));
@@ -547,12 +579,84 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
   __syncthreads();
 }
 
+// x-direction closure of one tile row (lane = x): h(p) = min(h(p), h(q) + |p - q|)
+// over the runs of residual arcs p -> p+1 -> ... -> q (axp) and p -> p-1 ->
+// ... -> q (axm), by doubling.  The arc runs are read from the row's arc
+// masks, so only the values move between lanes.
+__device__ __forceinline__ int row_close(int v, unsigned axp, unsigned axm, int lane) {
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int nv = __shfl_down_sync(FULL, v, off);
+    const unsigned run = (1u << off) - 1u;
+    if (lane + off < 32 && ((~axp >> lane) & run) == 0u) v = min(v, nv + off);
+  }
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int nv = __shfl_up_sync(FULL, v, off);
+    const unsigned run = (1u << off) - 1u;
+    if (lane >= off && ((~axm >> (lane - off + 1)) & run) == 0u) v = min(v, nv + off);
+  }
+  return v;
+}
+
+// In-tile closure of a warp's tile (lane = x, hv[i] = row i's height, lab[i]
+// its arc byte, AXP / AXM the rows' x-arc masks): h(u) = min(h(u), h(v) + 1)
+// over residual arcs u -> v inside the tile, to the fixpoint.  Row closures
+// by doubling shuffles, y and z runs in registers (a backward and a forward
+// sweep per line); bounded by the tile's nodes (every pass but the last
+// lowers some height, and heights are bounded below by 0).
+template <int DIMS, int TY, int TZ>
+__device__ __forceinline__ void tile_close(int (&hv)[TY * TZ], const unsigned (&lab)[TY * TZ],
+                                           const unsigned (&AXP)[TY * TZ], const unsigned (&AXM)[TY * TZ], int lane) {
+  constexpr int R = TY * TZ;
+  for (int pass = 0; pass < 32 * R; ++pass) {
+    bool ch = false;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int v = row_close(hv[i], AXP[i], AXM[i], lane);
+      ch |= v < hv[i];
+      hv[i] = v;
+    }
+#pragma unroll
+    for (int z = 0; z < TZ; ++z) {
+#pragma unroll
+      for (int y = TY - 2; y >= 0; --y) {
+        const int i = z * TY + y;
+        if ((lab[i] & jfc::A_YP) && hv[i + 1] + 1 < hv[i]) { hv[i] = hv[i + 1] + 1; ch = true; }
+      }
+#pragma unroll
+      for (int y = 1; y < TY; ++y) {
+        const int i = z * TY + y;
+        if ((lab[i] & jfc::A_YM) && hv[i - 1] + 1 < hv[i]) { hv[i] = hv[i - 1] + 1; ch = true; }
+      }
+    }
+    if constexpr (DIMS == 3) {
+#pragma unroll
+      for (int y = 0; y < TY; ++y) {
+#pragma unroll
+        for (int z = TZ - 2; z >= 0; --z) {
+          const int i = z * TY + y;
+          if ((lab[i] & jfc::A_ZP) && hv[i + TY] + 1 < hv[i]) { hv[i] = hv[i + TY] + 1; ch = true; }
+        }
+#pragma unroll
+        for (int z = 1; z < TZ; ++z) {
+          const int i = z * TY + y;
+          if ((lab[i] & jfc::A_ZM) && hv[i - TY] + 1 < hv[i]) { hv[i] = hv[i - TY] + 1; ch = true; }
+        }
+      }
+    }
+    if (!__any_sync(FULL, ch)) break;
+  }
+}
+
 // First pass of the global relabel, one warp per tile: a bit-parallel BFS
 // from the deficit nodes.  Each tile row is a 32-bit word (bit = lane); the
 // level-d frontier expands through the residual-arc masks in a few word
 // operations per row, so a tile costs (levels x rows) word ops and no block
 // barrier.  Halo nodes count as sources only when they are deficits
-// (h = 0 in this pass); everything later passes refine.
+// (h = 0 in this pass); everything later passes refine.  (A min-plus closure
+// of the tile instead of the level steps measured slower here: the deficits
+// lie close, so few levels run, and the pass streams its loads.)
 template <int DIMS, int TY, int TZ>
 __device__ __forceinline__ void relabel_first_warp(const TileSet& ts, int tid, const BfsQ& Q, int& cur_grid,
                                                    int& delta) {
@@ -850,26 +954,6 @@ __device__ __forceinline__ void relabel_frontier_warp(const TileSet& ts, int tid
   flag_neighbours<DIMS, TY, TZ>(g, a, tid, rows_changed, c0 != 0, c31 != 0, again, Q);
 }
 
-// x-direction closure of one tile row (lane = x): h(p) = min(h(p), h(q) + |p - q|)
-// over the runs of residual arcs p -> p+1 -> ... -> q (axp) and p -> p-1 ->
-// ... -> q (axm), by doubling.  The arc runs are read from the row's arc
-// masks, so only the values move between lanes.
-__device__ __forceinline__ int row_close(int v, unsigned axp, unsigned axm, int lane) {
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const int nv = __shfl_down_sync(FULL, v, off);
-    const unsigned run = (1u << off) - 1u;
-    if (lane + off < 32 && ((~axp >> lane) & run) == 0u) v = min(v, nv + off);
-  }
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const int nv = __shfl_up_sync(FULL, v, off);
-    const unsigned run = (1u << off) - 1u;
-    if (lane >= off && ((~axm >> (lane - off + 1)) & run) == 0u) v = min(v, nv + off);
-  }
-  return v;
-}
-
 // Frontier visit, one warp per tile, min-plus form: the tile's heights in
 // registers (lane = x, one register per row), lowered by the halo heights
 // across residual arcs, then closed in place: row closures by doubling
@@ -880,11 +964,10 @@ __device__ __forceinline__ int row_close(int v, unsigned axp, unsigned axm, int 
 // level.  Improvements at or above the distance cap are dropped (those
 // nodes stay unreachable).
 template <int DIMS, int TY, int TZ>
-__device__ __forceinline__ void relabel_frontier_minplus(const TileSet& ts, int tid, const BfsQ& Q, int& cur_grid,
-                                                         int& delta) {
+__device__ __forceinline__ void relabel_frontier_minplus(const TileSet& ts, int tid, int4 ti, const BfsQ& Q,
+                                                         int& cur_grid, int& delta) {
   constexpr int R = TY * TZ;
   const int lane = threadIdx.x & 31;
-  const int4 ti = ts.d_info[tid];
   const GridDev& g = ts.d_desc[ti.x];
   const Addr a = make_addr<DIMS, TY, TZ>(g, ti, lane);
   unsigned lab[R];
@@ -905,77 +988,56 @@ __device__ __forceinline__ void relabel_frontier_minplus(const TileSet& ts, int 
     if (lab[i] & 128u) posm |= 1u << i;
   }
   // the halo, fixed during the visit: y faces per z slice (lane = x), z
-  // faces per row y, x faces in lanes r (left of row r) and 16 + r (right)
+  // faces per row y, x faces in lanes r (left of row r) and 16 + r (right);
+  // loaded together with the tile (no load waits for the arc bytes)
+  int HT[TZ], HB[TZ], HZT[DIMS == 3 ? TY : 1], HZB[DIMS == 3 ? TY : 1];
+#pragma unroll
+  for (int z = 0; z < TZ; ++z) {
+    const long long n = roff<TY>(a, z * TY);
+    HT[z] = a.has_yT ? g.h[n - a.pitch] : JFC_INF;
+    HB[z] = a.has_yB ? g.h[n + (long long)TY * a.pitch] : JFC_INF;
+  }
+  if constexpr (DIMS == 3) {
+#pragma unroll
+    for (int y = 0; y < TY; ++y) {
+      const long long n = roff<TY>(a, y);
+      HZT[y] = a.has_zT ? g.h[n - a.slab] : JFC_INF;
+      HZB[y] = a.has_zB ? g.h[n + (long long)TZ * a.slab] : JFC_INF;
+    }
+  }
+  const int xrow = lane & 15;
+  int hx = JFC_INF;
+  if (xrow < R && (lane < 16 ? a.has_xL : a.has_xR))
+    hx = g.h[(long long)(lane < 16 ? a.x0 - 1 : a.x0 + 32) + (long long)(a.y0 + xrow % TY) * a.pitch +
+             (long long)(a.z0 + xrow / TY) * a.slab];
+  // the tile's interior is at its fixpoint (the dense pass or its last
+  // visit closed it, and only its own visits write it), so only a halo seed
+  // that lowers a border node can change anything
+  bool seeded = false;
+  auto seed = [&](int& v, bool arc, int hn) {
+    if (arc && hn + 1 < v) { v = hn + 1; seeded = true; }
+  };
 #pragma unroll
   for (int z = 0; z < TZ; ++z) {
     const int it = z * TY, ib = z * TY + TY - 1;
-    const long long n = roff<TY>(a, it);
-    if (a.has_yT && (lab[it] & jfc::A_YM)) hv[it] = min(hv[it], g.h[n - a.pitch] + 1);
-    if (a.has_yB && (lab[ib] & jfc::A_YP)) hv[ib] = min(hv[ib], g.h[n + (long long)TY * a.pitch] + 1);
+    seed(hv[it], lab[it] & jfc::A_YM, HT[z]);
+    seed(hv[ib], lab[ib] & jfc::A_YP, HB[z]);
   }
   if constexpr (DIMS == 3) {
 #pragma unroll
     for (int y = 0; y < TY; ++y) {
       const int it = y, ib = (TZ - 1) * TY + y;
-      const long long n = roff<TY>(a, y);
-      if (a.has_zT && (lab[it] & jfc::A_ZM)) hv[it] = min(hv[it], g.h[n - a.slab] + 1);
-      if (a.has_zB && (lab[ib] & jfc::A_ZP)) hv[ib] = min(hv[ib], g.h[n + (long long)TZ * a.slab] + 1);
+      seed(hv[it], lab[it] & jfc::A_ZM, HZT[y]);
+      seed(hv[ib], lab[ib] & jfc::A_ZP, HZB[y]);
     }
   }
-  {
-    const int xrow = lane & 15;
-    const bool left = lane < 16;
-    int hx = JFC_INF;
-    if (xrow < R && (left ? a.has_xL : a.has_xR))
-      hx = g.h[(long long)(left ? a.x0 - 1 : a.x0 + 32) + (long long)(a.y0 + xrow % TY) * a.pitch +
-               (long long)(a.z0 + xrow / TY) * a.slab];
 #pragma unroll
-    for (int i = 0; i < R; ++i) {
-      const int hl = __shfl_sync(FULL, hx, i), hr = __shfl_sync(FULL, hx, 16 + i);
-      if (lane == 0 && (lab[i] & jfc::A_XM)) hv[i] = min(hv[i], hl + 1);
-      if (lane == 31 && (lab[i] & jfc::A_XP)) hv[i] = min(hv[i], hr + 1);
-    }
+  for (int i = 0; i < R; ++i) {
+    const int hl = __shfl_sync(FULL, hx, i), hr = __shfl_sync(FULL, hx, 16 + i);
+    seed(hv[i], lane == 0 && (lab[i] & jfc::A_XM), hl);
+    seed(hv[i], lane == 31 && (lab[i] & jfc::A_XP), hr);
   }
-  // closure to the fixpoint (bounded by the tile's nodes: every pass but the
-  // last lowers some height, and heights are bounded below by 0)
-  for (int pass = 0; pass < 32 * R; ++pass) {
-    bool ch = false;
-#pragma unroll
-    for (int i = 0; i < R; ++i) {
-      const int v = row_close(hv[i], AXP[i], AXM[i], lane);
-      ch |= v < hv[i];
-      hv[i] = v;
-    }
-#pragma unroll
-    for (int z = 0; z < TZ; ++z) {
-#pragma unroll
-      for (int y = TY - 2; y >= 0; --y) {
-        const int i = z * TY + y;
-        if ((lab[i] & jfc::A_YP) && hv[i + 1] + 1 < hv[i]) { hv[i] = hv[i + 1] + 1; ch = true; }
-      }
-#pragma unroll
-      for (int y = 1; y < TY; ++y) {
-        const int i = z * TY + y;
-        if ((lab[i] & jfc::A_YM) && hv[i - 1] + 1 < hv[i]) { hv[i] = hv[i - 1] + 1; ch = true; }
-      }
-    }
-    if constexpr (DIMS == 3) {
-#pragma unroll
-      for (int y = 0; y < TY; ++y) {
-#pragma unroll
-        for (int z = TZ - 2; z >= 0; --z) {
-          const int i = z * TY + y;
-          if ((lab[i] & jfc::A_ZP) && hv[i + TY] + 1 < hv[i]) { hv[i] = hv[i + TY] + 1; ch = true; }
-        }
-#pragma unroll
-        for (int z = 1; z < TZ; ++z) {
-          const int i = z * TY + y;
-          if ((lab[i] & jfc::A_ZM) && hv[i - TY] + 1 < hv[i]) { hv[i] = hv[i - TY] + 1; ch = true; }
-        }
-      }
-    }
-    if (!__any_sync(FULL, ch)) break;
-  }
+  if (__any_sync(FULL, seeded)) tile_close<DIMS, TY, TZ>(hv, lab, AXP, AXM, lane);
   const int cap = jfc::cap_of(g, ts.d_ctr);
   unsigned rows_changed = 0;
   bool c0 = false, c31 = false, act_lo = false, act_hi = false;
@@ -1070,6 +1132,9 @@ __global__ void __launch_bounds__(256, (DIMS == 3 && TY * TZ > 8) ? 1 : (DIMS ==
   const int lane = threadIdx.x & 31;
   const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= ts.ntiles) return;
+  // (appends straight to the queue: gathering a CTA's appends behind a block
+  // barrier measured slower, the barrier holds the CTA's slot to its
+  // slowest warp)
   BfsQ Q{ts.d_flag_bfs[1], ts.d_q_bfs[1], &ctr->qn_bfs[1]};
   int wgrid = -1, wdelta = 0;
   relabel_first_warp<DIMS, TY, TZ>(ts, (int)w, Q, wgrid, wdelta);
@@ -1091,8 +1156,12 @@ __global__ void __launch_bounds__(256, (DIMS == 3 && TY * TZ > 8) ? 1 : (DIMS ==
 template <int DIMS, int TY, int TZ>
 __global__ void __launch_bounds__(256, JFC_RELABEL_MINPLUS ? (TY * TZ > 8 ? 2 : 3) : JFC_RELABEL_WARP_MINB)
     k_relabel_warp(TileSet ts, int max_passes) {
+  __shared__ int s_items[8][64];   // per-warp staged queue appends (at most 38 before a flush)
+  __shared__ int s_cnt[8];
   DevCounters* ctr = ts.d_ctr;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) s_cnt[warp] = 0;
+  __syncwarp();
   unsigned long long visits = 0;
   int cur_grid = -1, delta = 0;
   bool ok = true;
@@ -1106,19 +1175,55 @@ __global__ void __launch_bounds__(256, JFC_RELABEL_MINPLUS ? (TY * TZ > 8 ? 2 : 
       if (blockIdx.x == 0 && threadIdx.x == 0) ctr->bfs_status = 2;
       break;
     }
-    BfsQ Q{ts.d_flag_bfs[cb ^ 1], ts.d_q_bfs[cb ^ 1], &ctr->qn_bfs[cb ^ 1]};
+    BfsQ Q{ts.d_flag_bfs[cb ^ 1], ts.d_q_bfs[cb ^ 1], &ctr->qn_bfs[cb ^ 1], s_items[warp], &s_cnt[warp]};
     const int* queue = ts.d_q_bfs[cb];
     int* fcur = ts.d_flag_bfs[cb];
-    for (;;) {
-      const unsigned k = jfc::warp_ticket(&ctr->ticket[cb]);
-      if ((int)k >= n) break;
-      const int tt = queue[k];
+    // Tickets come in chunks of kChunk while the pass holds a full round of
+    // chunks beyond the warp's (one counter update per chunk: the ticket
+    // and queue counters are single addresses every warp updates, which
+    // serialises them), singly near the end of the pass.  The next ticket,
+    // its queue entry and its tile are fetched while the current tile is
+    // visited.  Queue appends are staged per warp and published 32 or more
+    // at a time.
+    constexpr unsigned kChunk = 4;
+    const long long round = (long long)gridDim.x * (blockDim.x >> 5);
+    unsigned k = 0, kend = 0;   // tickets [k, kend) held by the warp
+    auto take = [&]() -> int {
+      if (k >= kend) {
+        unsigned v = 0;
+        const unsigned c = jfc::vload((const int*)&ctr->ticket[cb]) + round * kChunk < (unsigned)n ? kChunk : 1u;
+        if (lane == 0) v = atomicAdd(&ctr->ticket[cb], c);
+        k = __shfl_sync(FULL, v, 0);
+        kend = k + c;
+      }
+      const unsigned kk = k++;
+      return (int)kk < n ? queue[kk] : -1;
+    };
+    int tt = take();
+    int4 ti = tt >= 0 ? ts.d_info[tt] : make_int4(0, 0, 0, 0);
+    while (tt >= 0) {
+      const int tn = take();
+      const int4 tin = tn >= 0 ? ts.d_info[tn] : make_int4(0, 0, 0, 0);
       if (lane == 0) fcur[tt] = 0;
       __syncwarp();
-      if (JFC_RELABEL_MINPLUS) relabel_frontier_minplus<DIMS, TY, TZ>(ts, tt, Q, cur_grid, delta);
+      if (JFC_RELABEL_MINPLUS) relabel_frontier_minplus<DIMS, TY, TZ>(ts, tt, ti, Q, cur_grid, delta);
       else relabel_frontier_warp<DIMS, TY, TZ>(ts, tt, Q, cur_grid, delta);
       ++visits;
+      __syncwarp();
+      if (*(volatile int*)Q.scnt >= 32) {
+        flush_staged(Q, lane);
+        __syncwarp();
+        if (lane == 0) *Q.scnt = 0;
+        __syncwarp();
+      }
+      tt = tn;
+      ti = tin;
     }
+    __syncwarp();
+    flush_staged(Q, lane);
+    __syncwarp();
+    if (lane == 0) *Q.scnt = 0;
+    __syncwarp();
     ok = jfc::grid_sync(ctr, [&]() {
       ctr->ticket[cb] = 0;
       ctr->qn_bfs[cb] = 0;
@@ -1247,8 +1352,8 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
       ctr->qn_bfs[cb] = 0;
       if (to_worklist) {
         ctr->wl_head = 0;
-        ctr->wl_tail = (unsigned)ctr->qn_bfs[cb ^ 1];
-        ctr->wl_out = ctr->qn_bfs[cb ^ 1];
+        const unsigned long long q = (unsigned)ctr->qn_bfs[cb ^ 1];
+        ctr->wl_tail_out = (q << 32) | q;
       }
     });
     if (to_worklist) { ++pass; break; }
@@ -1263,14 +1368,14 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
     const unsigned cap = (unsigned)ts.ntiles;
     int* ring = ts.d_q_bfs[0];          // the border check queued into buffer 0
     int* busy = ts.d_flag_bfs[1];       // free after the border check
-    const unsigned n0 = jfc::vload((const int*)&ctr->wl_tail);
+    const unsigned n0 = (unsigned)(*(volatile unsigned long long*)&ctr->wl_tail_out >> 32);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cap; i += (long long)gridDim.x * blockDim.x) {
       if (i >= n0) ring[i] = -1;
       busy[i] = 0;
     }
     ok = jfc::grid_sync(ctr, [&]() {});
     const unsigned long long max_spins = jfc::spin_cap(ctr);
-    const RlRing W{ring, cap, &ctr->wl_tail, &ctr->wl_out, &ctr->error, max_spins};
+    const RlRing W{ring, cap, &ctr->wl_tail_out, &ctr->error, max_spins};
     const BfsQ Q{ts.d_flag_bfs[0], nullptr, nullptr};
     while (ok) {
       if (threadIdx.x == 0) {
@@ -1281,19 +1386,17 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
         // count measures a stall (it restarts whenever the worklist moves:
         // items appended or finished), not the length of the relabel
         unsigned long long spins = 0;
-        unsigned seen_tail = jfc::vload((const int*)&ctr->wl_tail);
-        int seen_out = jfc::vload(&ctr->wl_out);
+        volatile unsigned long long* vto = &ctr->wl_tail_out;
+        unsigned long long seen = *vto;
         for (;;) {
           if (*(volatile int*)slot >= 0) {
             const int v = atomicExch(slot, -1);
             if (v >= 0) { tile = v; break; }
           }
-          const int out = jfc::vload(&ctr->wl_out);
-          if (out == 0 || *(volatile int*)&ctr->error) break;
-          const unsigned tl = (unsigned)jfc::vload((const int*)&ctr->wl_tail);
-          if (out != seen_out || tl != seen_tail) {
-            seen_out = out;
-            seen_tail = tl;
+          const unsigned long long to = *vto;
+          if ((unsigned)to == 0u || *(volatile int*)&ctr->error) break;
+          if (to != seen) {
+            seen = to;
             spins = 0;
           } else if (++spins > max_spins) {
             atomicExch(&ctr->error, 1);
@@ -1323,7 +1426,7 @@ __global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet
       if (threadIdx.x == 0) {
         __threadfence();
         atomicExch(busy + tt, 0);
-        atomicSub(&ctr->wl_out, 1);
+        if (!sm.folded) atomicAdd(&ctr->wl_tail_out, ~0ull);   // - 1 outstanding
       }
       if (threadIdx.x < 32) ++visits;
     }

@@ -41,17 +41,19 @@ METRIC = "Mnodes/s to exact min-cut (plain, 2D 4-conn 15000x10000 RGB)"
 
 
 def pr_traffic_per_visit():
-    """DRAM bytes per push-relabel tile visit from the committed summary of the
-    one-pass ncu capture of every push-relabel launch of a 4096x3072 solve
-    (under profiles/), or None; a full-size launch's traffic is this times its
-    visits (traffic grows with the visits: each reads and writes one tile)."""
-    try:
-        with open(os.path.join(ROOT, "profiles", "k_pr_phase_traffic_4096x3072.md")) as f:
-            for line in f:
-                if line.startswith("traffic_bytes_per_visit:"):
-                    return float(line.split(":")[1])
-    except OSError:
-        pass
+    """DRAM bytes per push-relabel tile visit, from the committed summary of the
+    one-pass ncu capture of every push-relabel launch of this workload's run
+    (profiles/k_pr_phase_traffic_15000x10000.md), else of a 4096x3072 run, or
+    None.  A launch's traffic is this times its visits (each visit reads and
+    writes one tile)."""
+    for name in ("k_pr_phase_traffic_15000x10000.md", "k_pr_phase_traffic_4096x3072.md"):
+        try:
+            with open(os.path.join(ROOT, "profiles", name)) as f:
+                for line in f:
+                    if line.startswith("traffic_bytes_per_visit:"):
+                        return float(line.split(":")[1])
+        except OSError:
+            pass
     return None
 
 
@@ -690,8 +692,9 @@ def main():
                          "algorithmic_bytes_per_launch": visits * bytes_per_visit / max(1, pr_launches),
                          "launches": pr_launches,
                          "kernel": "k_pr_phase (push-relabel phases; %d B per tile visit algorithmic, %s peak; "
-                                   "traffic: DRAM bytes per visit of the committed ncu capture of a 4096x3072 "
-                                   "solve times this workload's visits per launch)" % (bytes_per_visit, peak_kind)},
+                                   "traffic: DRAM bytes per visit of the committed one-pass ncu capture of "
+                                   "this workload's push-relabel launches times the visits per launch)"
+                                   % (bytes_per_visit, peak_kind)},
         }
         if world == 1 and not args.no_cpu_baseline:
             print("bench: cpu baseline", file=sys.stderr, flush=True)

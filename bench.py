@@ -426,14 +426,14 @@ def bench_serve(jfcut, torch, ctx, seconds=20.0, rate=200.0, budget_gb=96, max_c
             info = srv.wait(sid, 300000)
             with lock:
                 state["cold_out"] -= 1
-            rec = [("cold", s["dims"], s["n"], info.ms_total, info.status)]
+            rec = [("cold", s["dims"], s["n"], info.ms_total, info.status, info.ms_queue, info.ms_solve)]
             flow = info.flow
             for idx, ns in s["strokes"][:k]:
                 if info.status:
                     break
                 srv.edit(sid, idx, ns)
                 info = srv.wait(sid, 300000)
-                rec.append(("warm", s["dims"], s["n"], info.ms_total, info.status))
+                rec.append(("warm", s["dims"], s["n"], info.ms_total, info.status, info.ms_queue, info.ms_solve))
                 flow = info.flow
             srv.close_session(sid)
             with lock:
@@ -483,8 +483,13 @@ def bench_serve(jfcut, torch, ctx, seconds=20.0, rate=200.0, budget_gb=96, max_c
         g.close()
 
     def lat(kind, dims):
-        v = [r[3] for r in records if r[0] == kind and r[1] == dims and r[4] == 0]
-        return {"n": len(v), "p50_ms": pct(v, 50), "p99_ms": pct(v, 99)}
+        rs = [r for r in records if r[0] == kind and r[1] == dims and r[4] == 0]
+        v = [r[3] for r in rs]
+        # the server's split of a request's latency: waiting for admission
+        # (queue) and admitted until its result (solve, sharing the GPU)
+        return {"n": len(v), "p50_ms": pct(v, 50), "p99_ms": pct(v, 99),
+                "queue_p50_ms": pct([r[5] for r in rs], 50), "queue_p99_ms": pct([r[5] for r in rs], 99),
+                "solve_p50_ms": pct([r[6] for r in rs], 50), "solve_p99_ms": pct([r[6] for r in rs], 99)}
 
     ok = [r for r in records if r[4] == 0]
     served_nodes = sum(r[2] for r in ok)

@@ -105,7 +105,9 @@ typedef struct jfc_params {
   int pr_sched;          /* scheduling of the push-relabel visits between two global relabels:
                             1 = checkerboard parity sweeps with a grid barrier between colours,
                             2 = an asynchronous worklist with per-tile neighbour exclusion (no
-                            barriers), 0 = automatic.  Same arithmetic, same results */
+                            barriers), 3 = sweeps while more than 1/256 of the tiles are active
+                            and the worklist in the tail, 0 = automatic.  Same arithmetic, same
+                            results */
   int local_iters_tail;  /* push/relabel rounds per visit once fewer than 1/256 of the tiles are
                             active (the long-path tail of a solve, where excess has to cross
                             whole tiles): 0 = automatic, < 0 = local_iters */
@@ -268,6 +270,8 @@ typedef struct jfc_request_info {
   int warm;                              /* 1 if re-solved from resident state */
 } jfc_request_info;
 
+/* max_slots: requests solving at once (0: 64); cold requests take at most
+ * max_slots - max_slots / 4 of them, the rest stay free for warm edits. */
 int  jfc_server_create(jfc_ctx* ctx, size_t hbm_budget_bytes, int max_slots, jfc_server** out);
 void jfc_server_destroy(jfc_server* s);
 /* Submit a new session from host image + seeds; returns a session id >= 0 in *sid. */

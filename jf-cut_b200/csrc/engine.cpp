@@ -87,6 +87,8 @@ bool pr_split_for(const jfc_params& p, int dims) { return dims == 2 && p.tile_ro
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// (blocks from the stream-ordered allocator are freed without a device
+// synchronisation: nothing may still run on them)
 void tileset_free(TileSet& ts) {
   tileset_drop_graphs(ts);
   if (ts.d_block) cudaFree(ts.d_block);
@@ -217,7 +219,16 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const st
   // tile sets between relabels); otherwise allocate with headroom when asked
   // to stage asynchronously
   if (!ts.d_block || ts.cap_tiles < ntiles || ts.cap_grids < ngrids) {
-    tileset_free(ts);
+    if (s) {
+      // stream-ordered: the old block goes back to the pool when `s` reaches
+      // the free, and nothing waits for the other streams' work (the server
+      // grows its tile sets while builds run); the pinned staging is kept
+      tileset_drop_graphs(ts);
+      if (ts.d_block) JFC_CUDA(cudaFreeAsync(ts.d_block, s));
+      ts.d_block = nullptr;
+    } else {
+      tileset_free(ts);
+    }
     ts.cap_tiles = s ? ntiles + ntiles / 4 + 64 : ntiles;
     ts.cap_grids = s ? ngrids + ngrids / 4 + 8 : ngrids;
     if (ts.cap_tiles < 1) ts.cap_tiles = 1;
@@ -225,7 +236,8 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const st
     size_t total = 0;
     tileset_carve(ts, nullptr, &total);
     char* blk = nullptr;
-    JFC_CUDA(cudaMalloc((void**)&blk, total));
+    if (s) JFC_CUDA(cudaMallocAsync((void**)&blk, total, s));
+    else JFC_CUDA(cudaMalloc((void**)&blk, total));
     ts.d_block = blk;
     ts.block_bytes = total;
     tileset_carve(ts, blk, &total);
@@ -453,14 +465,13 @@ static cudaGraphExec_t cycle_graph(TileSet& ts, const int* pin_sw, int local_ite
 // One relabel cycle, replayed from a graph when enabled; returns the outcome
 // of its global relabel.
 static int run_cycle(jfc_ctx* ctx, TileSet& ts, const jfc_params& p, int interval, int h_cap, int local_iters,
-                     int& passes, std::vector<int>& active, int* sweeps_done, bool* used_graph) {
+                     int sched, int& passes, std::vector<int>& active, int* sweeps_done, bool* used_graph) {
   cudaStream_t s = ctx->stream;
   int rc = pin_reserve(ctx, pin_need_cycle(ts));
   if (rc) return rc;
   int* pin_sw = pin_sweeps(ctx, ts);
   pin_sw[0] = interval;   // the previous cycle's copies finished at its sync
   pin_sw[1] = h_cap;
-  const int sched = pr_sched_for(p);
   cudaGraphExec_t x = p.use_graph ? cycle_graph(ts, pin_sw, local_iters, p.max_bfs_passes, sched, s, ctx->h_pin)
                                   : nullptr;
   if (x) {
@@ -590,7 +601,9 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
       // excess crosses a whole tile per visit instead of per several sweeps
       const bool tail = total() * 256 < (long long)ts.ntiles;
       const int li = tail ? tail_iters : p.local_iters;
-      rc = run_cycle(ctx, ts, p, interval, h_cap, li, st.bfs_passes, active, &sw, &graphs);
+      // pr_sched 3: parity sweeps in the bulk, the worklist in the tail
+      const int sched = pr_sched_for(p) == 3 ? (tail ? 2 : 1) : pr_sched_for(p);
+      rc = run_cycle(ctx, ts, p, interval, h_cap, li, sched, st.bfs_passes, active, &sw, &graphs);
       last_cap = h_cap;
       ++st.pr_phases;
       if (rc) return rc;

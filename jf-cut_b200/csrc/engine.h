@@ -42,8 +42,6 @@ struct jfc_graph {
   TileSet ts;                    // tile set of this graph alone
   int ts_shape = -1;             // tile shape the tile set was built for
   DevModel model;
-  uint8_t* d_dense = nullptr;    // dense scratch for pack / unpack (lazily)
-  size_t dense_bytes = 0;
   jfc_stats last{};
 };
 
@@ -85,9 +83,10 @@ bool pr_split_for(const jfc_params& p, int dims);
 inline int interval_for(const jfc_params& p, int dims) {
   return p.relabel_interval > 0 ? p.relabel_interval : (dims == 2 ? 2 : 3);
 }
-// Push-relabel visit scheduling (1 sweeps, 2 worklist): pr_sched, or the
-// measured default when it is 0.
-inline int pr_sched_for(const jfc_params& p) { return p.pr_sched == 1 || p.pr_sched == 2 ? p.pr_sched : 1; }
+// Push-relabel visit scheduling (1 sweeps, 2 worklist, 3 sweeps while many
+// tiles are active and the worklist in the tail): pr_sched, or the measured
+// default when it is 0.
+inline int pr_sched_for(const jfc_params& p) { return p.pr_sched >= 1 && p.pr_sched <= 3 ? p.pr_sched : 1; }
 // Distance cap of the global relabels while solving (0: none): relabel_cap,
 // or when it is 0 the measured default per dimensionality.  The Fast-Cut
 // comparison mode keeps the reference's exact relabels.
@@ -112,6 +111,10 @@ size_t state_bytes(int dims, int w, int h, int d);
 void model_defaults(jfc_model& m);
 int build_core(jfc_graph* G, const void* img, int pixfmt, const uint8_t* seeds, const jfc_model* mdl,
                cudaMemcpyKind kind);
+// Free a graph whose last use was ordered on stream `s` (or completed) without
+// synchronising the device: its memory goes back to the pool when `s` reaches
+// the free (the server's solver thread, while other streams keep running).
+void graph_release(jfc_graph* G, cudaStream_t s);
 // Copy a dense array into (to_dense false) or out of a padded plane of G.
 cudaError_t copy_plane(void* padded, const void* dense, size_t elem, const jfc_graph* G, bool to_dense,
                        cudaMemcpyKind kind, cudaStream_t s);

@@ -86,6 +86,7 @@ struct jfc_server {
   jfc_ctx* solve_ctx = nullptr;
   jfc_ctx* build_ctx = nullptr;
   cudaStream_t read_stream = nullptr;
+  cudaStream_t solve_stream = nullptr;   // the solver context's stream (highest priority)
   std::mutex read_mu;
   size_t budget = 0, used = 0;
   int max_slots = 64;
@@ -143,10 +144,16 @@ void cancel_all(jfc_server* S, Session* s, Clock::time_point now) {
 
 // Release a session's device state and budget (solver thread; no tile set
 // references its grid any more).  Label reads hold read_mu while they copy.
+// Called by the solver thread only, for a session in no tile set: its last
+// kernels ran on the solver stream (before a read-back the thread waited
+// for), its build finished on the builder stream before it was handed over,
+// and read_mu keeps label reads out, so the release is ordered on the solver
+// stream and synchronises nothing else (a device-wide wait here would stall
+// the solver for the builder's work in flight).
 void free_session(jfc_server* S, Session* s) {
   std::lock_guard<std::mutex> rl(S->read_mu);
   if (s->G) {
-    jfc_graph_destroy(s->G);
+    graph_release(s->G, S->solve_ctx->stream);
     s->G = nullptr;
   }
   std::lock_guard<std::mutex> lk(S->mu);
@@ -413,19 +420,32 @@ void solver_loop(jfc_server* S) {
   constexpr long long kBulkNodes = 1ll << 28;
   constexpr int kBulkPairsBusy = 2;
   auto nodes_of = [](const Session* s) { return (long long)s->w * s->h * s->d; };
-  for (;;) {
-    // admission: requests waiting for a slot join their lane at its next relabel
+  // admission: requests waiting for a slot join their lane at its next
+  // relabel.  Runs at the top of every round and again between interactive
+  // cycles (an edit that arrives during a round does not wait for the round
+  // to end); `idle_wait` blocks while every lane is empty.  Returns false
+  // when the server stops.
+  auto admit = [&](bool idle_wait) -> bool {
     std::vector<Session*> admitted, frees;
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      if (lanes[0].empty() && lanes[1].empty() && lanes[2].empty())
+      if (idle_wait && lanes[0].empty() && lanes[1].empty() && lanes[2].empty())
         S->cv_work.wait(lk, [&] { return S->stop || !S->ready_q.empty() || !S->to_free.empty(); });
-      if (S->stop) break;
+      if (S->stop) return false;
+      if (!idle_wait && S->ready_q.empty() && S->to_free.empty()) return true;
       const Clock::time_point now = Clock::now();
       frees.swap(S->to_free);   // idle sessions: in no lane
       int members = 0;
       for (Lane& L : lanes) members += (int)(L.mem[0].size() + L.mem[1].size() + L.joining.size());
       int slots = S->max_slots - members;
+      // a quarter of the slots stays free for edits: cold requests take at
+      // most the rest, so a warm edit never waits for a bulk solve to finish
+      // before it is admitted
+      const int bulk_slots = std::max(1, S->max_slots - std::max(1, S->max_slots / 4));
+      int bulk_members = (int)lanes[kBulk].joining.size();
+      for (int k = 0; k < 2; ++k)
+        for (const Member& m : lanes[kBulk].mem[k])
+          if (!m.done) ++bulk_members;
       long long bulk_nodes = 0;
       for (int k = 0; k < 2; ++k)
         for (const Member& m : lanes[kBulk].mem[k])
@@ -440,12 +460,16 @@ void solver_loop(jfc_server* S) {
         const int sid = S->ready_q.front();
         S->ready_q.pop_front();
         const bool cold = !s->reqs.empty() && s->reqs.front().cold && !s->cancel;
-        if (cold && (bulk_full || (bulk_nodes > 0 && bulk_nodes + nodes_of(s) > kBulkNodes))) {
+        if (cold && (bulk_full || bulk_members >= bulk_slots ||
+                     (bulk_nodes > 0 && bulk_nodes + nodes_of(s) > kBulkNodes))) {
           bulk_full = true;
           keep.push_back(sid);
           continue;
         }
-        if (cold) bulk_nodes += nodes_of(s);
+        if (cold) {
+          bulk_nodes += nodes_of(s);
+          ++bulk_members;
+        }
         if (s->cancel || s->reqs.empty()) {
           cancel_all(S, s, now);
           s->phase = IDLE;
@@ -463,7 +487,7 @@ void solver_loop(jfc_server* S) {
         S->ready_q.push_front(keep.back());
         keep.pop_back();
       }
-      ++S->loops;
+      if (idle_wait) ++S->loops;
     }
     for (Session* s : frees) {
       free_session(S, s);
@@ -501,6 +525,10 @@ void solver_loop(jfc_server* S) {
       S->solving = solving;
       S->peak_solving = std::max(S->peak_solving, solving);
     }
+    return true;
+  };
+  for (;;) {
+    if (!admit(true)) break;
     // interactive lane first (until it drains, bounded), then one bulk cycle
     auto fail_all = [&](int rc) { for (Lane& L : lanes) fail_lane(S, L, rc); };
     // edits first (until they drain, bounded): small-edit cycles, with a
@@ -513,6 +541,7 @@ void solver_loop(jfc_server* S) {
         const int rc = lane_cycle(S, lanes[kSmall], kSmall);
         if (rc) { fail_all(rc); return; }
       }
+      if (!admit(false)) break;
       if (large && (!small || c % kLargeEvery == kLargeEvery - 1)) {
         const int rc = lane_cycle(S, lanes[kLarge], kLarge, small ? kBulkPairsBusy : 1 << 30);
         if (rc) { fail_all(rc); return; }
@@ -563,9 +592,23 @@ int jfc_server_create(jfc_ctx* ctx, size_t hbm_budget_bytes, int max_slots, jfc_
   if (rc == JFC_OK) rc = jfc_create(ctx->device, &S->params, &S->build_ctx);
   if (rc == JFC_OK && cudaStreamCreateWithFlags(&S->read_stream, cudaStreamNonBlocking) != cudaSuccess)
     rc = set_error(JFC_ERR_CUDA, "cudaStreamCreate");
+  // the solver's launches get the device's highest stream priority: its
+  // persistent phases need every SM at once, and the builder's kernels
+  // (capacity builds and k-means of large volumes) would otherwise keep
+  // taking the SMs that free up while a phase waits to start
+  if (rc == JFC_OK) {
+    int lo = 0, hi = 0;
+    if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&S->solve_stream, cudaStreamNonBlocking, hi) != cudaSuccess)
+      rc = set_error(JFC_ERR_CUDA, "cudaStreamCreateWithPriority");
+    else
+      rc = jfc_set_stream(S->solve_ctx, S->solve_stream);
+  }
   if (rc != JFC_OK) {
     if (S->solve_ctx) jfc_destroy(S->solve_ctx);
     if (S->build_ctx) jfc_destroy(S->build_ctx);
+    if (S->read_stream) cudaStreamDestroy(S->read_stream);
+    if (S->solve_stream) cudaStreamDestroy(S->solve_stream);
     return rc;
   }
   jfc_server* raw = S.release();
@@ -586,6 +629,7 @@ void jfc_server_destroy(jfc_server* S) {
   S->builder.join();
   S->solver.join();
   cudaSetDevice(S->device);
+  cudaDeviceSynchronize();   // the threads' last frees and launches complete first
   for (int k = 0; k < 2; ++k) tileset_free(S->cut_ts[k]);
   for (auto& kv : S->sessions)
     if (kv.second->G) jfc_graph_destroy(kv.second->G);
@@ -593,6 +637,7 @@ void jfc_server_destroy(jfc_server* S) {
   if (S->read_stream) cudaStreamDestroy(S->read_stream);
   jfc_destroy(S->solve_ctx);
   jfc_destroy(S->build_ctx);
+  if (S->solve_stream) cudaStreamDestroy(S->solve_stream);
   delete S;
 }
 
@@ -613,11 +658,13 @@ int jfc_server_submit(jfc_server* S, int dims, int w, int h, int d, const void* 
   if (model) s->model = *model;
   model_defaults(s->model);
   s->charge = session_bytes(dims, w, h, d, pixfmt, nseeds);
-  std::lock_guard<std::mutex> lk(S->mu);
-  if (S->fatal) return set_error(S->fatal, "server stopped after a device error");
   if (s->charge > S->budget) return set_error(JFC_ERR_OOM, "session needs more device memory than the server budget");
+  // the copies (up to hundreds of MB) are made before the server lock is
+  // taken: the solver thread takes it between every two relabel cycles
   s->img.assign((const uint8_t*)img, (const uint8_t*)img + n * jfc_pix_bytes(pixfmt));
   s->seeds.assign(seeds, seeds + n);
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (S->fatal) return set_error(S->fatal, "server stopped after a device error");
   Request r;
   r.cold = true;
   r.t_submit = Clock::now();
@@ -632,17 +679,23 @@ int jfc_server_submit(jfc_server* S, int dims, int w, int h, int d, const void* 
 
 int jfc_server_edit(jfc_server* S, int sid, const uint32_t* idx, const uint8_t* new_seed, size_t n) {
   if (!S || (n && (!idx || !new_seed))) return set_error(JFC_ERR_INVALID_ARG, "null argument");
+  // the edit is copied and its seed values checked before the server lock
+  // is taken (the solver thread takes it between every two relabel cycles)
+  Request r;
+  r.cold = false;
+  r.idx.assign(idx, idx + n);
+  r.seed.assign(new_seed, new_seed + n);
+  uint32_t max_idx = 0;
+  for (size_t j = 0; j < n; ++j) {
+    if (new_seed[j] > 2) return set_error(JFC_ERR_INVALID_ARG, "bad edit");
+    max_idx = std::max(max_idx, idx[j]);
+  }
   std::lock_guard<std::mutex> lk(S->mu);
   Session* s = find(S, sid);
   if (!s) return set_error(JFC_ERR_INVALID_ARG, "unknown session");
   if (s->phase == DEAD) return set_error(JFC_ERR_STATE, "session has no graph (build failed or cancelled)");
   const unsigned long long N = (unsigned long long)s->w * s->h * s->d;
-  for (size_t j = 0; j < n; ++j)
-    if (idx[j] >= N || new_seed[j] > 2) return set_error(JFC_ERR_INVALID_ARG, "bad edit");
-  Request r;
-  r.cold = false;
-  r.idx.assign(idx, idx + n);
-  r.seed.assign(new_seed, new_seed + n);
+  if (n && max_idx >= N) return set_error(JFC_ERR_INVALID_ARG, "bad edit");
   r.t_submit = Clock::now();
   s->cancel = false;
   s->reqs.push_back(std::move(r));

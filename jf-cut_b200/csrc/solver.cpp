@@ -98,11 +98,14 @@ int ensure_model_buffers(jfc_graph* G, int pixfmt) {
   DevModel& M = G->model;
   const size_t n = (size_t)G->W * G->H * G->D;
   const size_t ib = n * jfc_pix_bytes(pixfmt);
-  if (M.d_img && M.img_bytes != ib) { cudaFree(M.d_img); M.d_img = nullptr; }
-  if (!M.d_img) { JFC_CUDA(cudaMalloc(&M.d_img, ib)); M.img_bytes = ib; }
-  if (!M.d_seeds) JFC_CUDA(cudaMalloc((void**)&M.d_seeds, n));
-  if (!M.d_lut_s) JFC_CUDA(cudaMalloc((void**)&M.d_lut_s, sizeof(int) * (JFC_TQ + 1)));
-  if (!M.d_lut_t) JFC_CUDA(cudaMalloc((void**)&M.d_lut_t, sizeof(int) * (JFC_TQ + 1)));
+  // stream-ordered allocations (no device-wide synchronisation when a server
+  // frees a session while other work runs)
+  cudaStream_t s = G->ctx->stream;
+  if (M.d_img && M.img_bytes != ib) { JFC_CUDA(cudaFreeAsync(M.d_img, s)); M.d_img = nullptr; }
+  if (!M.d_img) { JFC_CUDA(cudaMallocAsync(&M.d_img, ib, s)); M.img_bytes = ib; }
+  if (!M.d_seeds) JFC_CUDA(cudaMallocAsync((void**)&M.d_seeds, n, s));
+  if (!M.d_lut_s) JFC_CUDA(cudaMallocAsync((void**)&M.d_lut_s, sizeof(int) * (JFC_TQ + 1), s));
+  if (!M.d_lut_t) JFC_CUDA(cudaMallocAsync((void**)&M.d_lut_t, sizeof(int) * (JFC_TQ + 1), s));
   return JFC_OK;
 }
 
@@ -234,13 +237,13 @@ int set_core(jfc_graph* G, const int32_t* e, const int32_t* const* ncap, int64_t
   JFC_CUDA(copy_plane(G->g.e, e, 4, G, false, kind, s));
   for (int k = 0; k < G->conn; ++k) JFC_CUDA(copy_plane(G->g.r[k], ncap[k], 4, G, false, kind, s));
   int* d_bad = nullptr;
-  JFC_CUDA(cudaMalloc((void**)&d_bad, sizeof(int)));
+  JFC_CUDA(cudaMallocAsync((void**)&d_bad, sizeof(int), s));
   JFC_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
   cudaError_t err = launch_fix_boundary(G->g, G->conn, d_bad, s);
   int bad = 0;
   if (err == cudaSuccess) err = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-  cudaFree(d_bad);
+  cudaFreeAsync(d_bad, s);
   if (err != cudaSuccess) return cuda_status(err, "graph set");
   if (bad) return set_error(JFC_ERR_INVALID_ARG, "negative n-link capacity");
   int rc = ensure_tileset(G);
@@ -377,11 +380,13 @@ int jfc_graph_create_grid(jfc_ctx* c, int dims, int w, int h, int d, int conn, j
   grid_layout(dims, w, h, d, pitch, Hp, Dp);
   const size_t plane = (size_t)pitch * Hp * Dp;
   G->state_bytes = state_bytes(dims, w, h, d);
-  cudaError_t e = cudaMalloc(&G->d_state, G->state_bytes);
+  // stream-ordered allocation on the context's stream (its release never
+  // synchronises the device, see graph_release), zeroed there, ordered
+  // before every later use of it
+  cudaError_t e = cudaMallocAsync(&G->d_state, G->state_bytes, c->stream);
   if (e != cudaSuccess) { delete G; return cuda_status(e, "graph allocation"); }
-  // zeroed on the context's stream, ordered before every later use of it
   e = cudaMemsetAsync(G->d_state, 0, G->state_bytes, c->stream);
-  if (e != cudaSuccess) { cudaFree(G->d_state); delete G; return cuda_status(e, "graph clear"); }
+  if (e != cudaSuccess) { cudaFreeAsync(G->d_state, c->stream); delete G; return cuda_status(e, "graph clear"); }
   char* p = (char*)G->d_state;
   GridDev& g = G->g;
   std::memset(&g, 0, sizeof(g));
@@ -400,7 +405,8 @@ int jfc_graph_create_grid(jfc_ctx* c, int dims, int w, int h, int d, int conn, j
 
 void jfc_graph_destroy(jfc_graph* G) {
   if (!G) return;
-  // the context may already be gone: use only what the graph owns
+  // the context may already be gone: use only what the graph owns; nothing
+  // may still run on the graph's memory when it goes back to the pool
   cudaSetDevice(G->device);
   cudaDeviceSynchronize();
   tileset_free(G->ts);
@@ -409,9 +415,23 @@ void jfc_graph_destroy(jfc_graph* G) {
   if (G->model.d_seeds) cudaFree(G->model.d_seeds);
   if (G->model.d_lut_s) cudaFree(G->model.d_lut_s);
   if (G->model.d_lut_t) cudaFree(G->model.d_lut_t);
-  if (G->d_dense) cudaFree(G->d_dense);
   delete G;
 }
+
+}  // extern "C"
+
+void graph_release(jfc_graph* G, cudaStream_t s) {
+  if (!G) return;
+  tileset_free(G->ts);
+  if (G->d_state) cudaFreeAsync(G->d_state, s);
+  if (G->model.d_img) cudaFreeAsync(G->model.d_img, s);
+  if (G->model.d_seeds) cudaFreeAsync(G->model.d_seeds, s);
+  if (G->model.d_lut_s) cudaFreeAsync(G->model.d_lut_s, s);
+  if (G->model.d_lut_t) cudaFreeAsync(G->model.d_lut_t, s);
+  delete G;
+}
+
+extern "C" {
 
 int jfc_graph_build_from_image(jfc_graph* g, const void* img, int pixfmt, const uint8_t* seeds,
                                const jfc_model* model) {

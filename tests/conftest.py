@@ -112,7 +112,7 @@ def _default_schedule(request):
 # explicitly.
 SCHEDULES = {"default": {}, "rows16": dict(tile_rows=16), "whole16": dict(tile_rows=16, pr_mode=2),
              "exact": dict(relabel_cap=-1), "cap2": dict(relabel_cap=2),
-             "sweeps": dict(pr_sched=1), "worklist": dict(pr_sched=2),
+             "sweeps": dict(pr_sched=1), "worklist": dict(pr_sched=2), "hybrid": dict(pr_sched=3),
              "rows16_sweeps": dict(tile_rows=16, pr_sched=1)}
 
 

@@ -87,6 +87,9 @@ struct jfc_server {
   jfc_ctx* build_ctx = nullptr;
   cudaStream_t read_stream = nullptr;
   cudaStream_t solve_stream = nullptr;   // the solver context's stream (highest priority)
+  Clock::time_point t0 = Clock::now();   // (verbose logs) server start
+  cudaMemPool_t pool = nullptr;          // the device's default pool (graph memory)
+  unsigned long long pool_threshold0 = 0;   // its release threshold before the server
   std::mutex read_mu;
   size_t budget = 0, used = 0;
   int max_slots = 64;
@@ -164,6 +167,12 @@ void free_session(jfc_server* S, Session* s) {
 
 void builder_loop(jfc_server* S) {
   cudaSetDevice(S->device);
+  // pinned staging of the image and seeds: the build's uploads run as plain
+  // DMA copies instead of the driver's staged copies from pageable memory
+  // (grown to the largest request seen, reused after each build's sync)
+  void* pin = nullptr;
+  size_t pin_bytes = 0;
+  struct PinFree { void*& p; ~PinFree() { if (p) cudaFreeHost(p); } } pin_free{pin};
   for (;;) {
     Session* s = nullptr;
     {
@@ -184,8 +193,32 @@ void builder_loop(jfc_server* S) {
       s->reqs.front().t_admit = Clock::now();
     }
     jfc_graph* G = nullptr;
+    const Clock::time_point tb = Clock::now();
+    const void* img = s->img.data();
+    const uint8_t* seeds = s->seeds.data();
+    const size_t need = align256(s->img.size()) + s->seeds.size();
+    if (need > pin_bytes) {
+      if (pin) cudaFreeHost(pin);
+      pin = nullptr;
+      pin_bytes = 0;
+      if (cudaMallocHost(&pin, need + need / 4) == cudaSuccess) pin_bytes = need + need / 4;
+      else pin = nullptr;   // no pinned memory: the pageable copies still work
+    }
+    if (pin) {
+      std::memcpy(pin, s->img.data(), s->img.size());
+      std::memcpy((char*)pin + align256(s->img.size()), s->seeds.data(), s->seeds.size());
+      img = pin;
+      seeds = (const uint8_t*)pin + align256(s->img.size());
+    }
     int rc = jfc_graph_create_grid(S->build_ctx, s->dims, s->w, s->h, s->d, s->dims == 2 ? 4 : 6, &G);
-    if (rc == JFC_OK) rc = build_core(G, s->img.data(), s->pixfmt, s->seeds.data(), &s->model, cudaMemcpyHostToDevice);
+    if (rc == JFC_OK) rc = build_core(G, img, s->pixfmt, seeds, &s->model, cudaMemcpyHostToDevice);
+    cudaStreamSynchronize(S->build_ctx->stream);   // the staging is free again, whatever the outcome
+    if (S->params.verbose) {
+      const Clock::time_point te = Clock::now();
+      auto ms = [](Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+      fprintf(stderr, "{\"build\": %d, \"nodes\": %lld, \"ms\": %.3f, \"t_end_ms\": %.1f}\n", s->sid,
+              (long long)s->w * s->h * s->d, ms(tb, te), ms(S->t0, te));
+    }
     std::unique_lock<std::mutex> lk(S->mu);
     s->G = G;
     std::vector<uint8_t>().swap(s->img);
@@ -303,8 +336,10 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id, int max_interval = 1 << 30) 
   }
   L.joining.clear();
   // 3. global relabel over the (re-formed) set
+  double ms_build = 0.0, ms_bfs = 0.0;   // (verbose) tile-set builds; phase + relabel to its read-back
   for (int k = 0; k < 2; ++k) {
     if (k == 0) t_form = Clock::now();
+    const Clock::time_point t_k = Clock::now();
     if (L.mem[k].empty()) {
       L.active[k].clear();
       continue;
@@ -316,9 +351,12 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id, int max_interval = 1 << 30) 
                              pr_split_for(p, k ? 3 : 2));
       if (rc) return rc;
     }
+    const Clock::time_point t_built = Clock::now();
     int passes = 0, sw = 0;
     int rc = engine_bfs(ctx, L.ts[k], p, false, passes, &L.active[k], nullptr, &sw);
     if (rc) return rc;
+    ms_build += std::chrono::duration<double, std::milli>(t_built - t_k).count();
+    ms_bfs += std::chrono::duration<double, std::milli>(Clock::now() - t_built).count();
     if (ran_pr[k])
       for (Member& m : L.mem[k]) m.s->sweeps += sw;
   }
@@ -389,10 +427,11 @@ int lane_cycle(jfc_server* S, Lane& L, int lane_id, int max_interval = 1 << 30) 
     const Clock::time_point t_end = Clock::now();
     auto ms = [](Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
     fprintf(stderr, "{\"lane\": \"%s\", \"members\": %zu, \"active_tiles\": %lld, \"tiles\": %lld, \"interval\": %d, "
-                    "\"ms_phase_membership\": %.3f, \"ms_form_relabel\": %.3f, \"ms_cut\": %.3f}\n",
+                    "\"ms_phase_membership\": %.3f, \"ms_form_relabel\": %.3f, \"ms_build\": %.3f, \"ms_bfs\": %.3f, "
+                    "\"ms_cut\": %.3f, \"t_end_ms\": %.1f}\n",
             lane_id == 0 ? "interactive" : lane_id == 1 ? "interactive-large" : "bulk",
             L.mem[0].size() + L.mem[1].size(), still, nt, L.interval,
-            ms(t_start, t_form), ms(t_form, t_relabel), ms(t_relabel, t_end));
+            ms(t_start, t_form), ms(t_form, t_relabel), ms_build, ms_bfs, ms(t_relabel, t_end), ms(S->t0, t_end));
   }
   if (still > 0 && still * 256 < nt) L.interval = std::min(L.interval * 2, p.relabel_interval_max);
   else L.interval = interval_for(p, 2);
@@ -611,6 +650,15 @@ int jfc_server_create(jfc_ctx* ctx, size_t hbm_budget_bytes, int max_slots, jfc_
     if (S->solve_stream) cudaStreamDestroy(S->solve_stream);
     return rc;
   }
+  // graph memory comes from the device's default pool (stream-ordered): keep
+  // up to the budget mapped in the pool between sessions, so a new session's
+  // allocation reuses memory instead of mapping fresh pages while the solver's
+  // kernels run (restored when the server goes)
+  if (cudaDeviceGetDefaultMemPool(&S->pool, S->device) == cudaSuccess) {
+    cudaMemPoolGetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &S->pool_threshold0);
+    unsigned long long thr = std::max<unsigned long long>(S->pool_threshold0, S->budget);
+    cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
   jfc_server* raw = S.release();
   raw->builder = std::thread(builder_loop, raw);
   raw->solver = std::thread(solver_loop, raw);
@@ -638,6 +686,10 @@ void jfc_server_destroy(jfc_server* S) {
   jfc_destroy(S->solve_ctx);
   jfc_destroy(S->build_ctx);
   if (S->solve_stream) cudaStreamDestroy(S->solve_stream);
+  if (S->pool) {
+    cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &S->pool_threshold0);
+    cudaMemPoolTrimTo(S->pool, 0);
+  }
   delete S;
 }
 

@@ -167,12 +167,6 @@ void free_session(jfc_server* S, Session* s) {
 
 void builder_loop(jfc_server* S) {
   cudaSetDevice(S->device);
-  // pinned staging of the image and seeds: the build's uploads run as plain
-  // DMA copies instead of the driver's staged copies from pageable memory
-  // (grown to the largest request seen, reused after each build's sync)
-  void* pin = nullptr;
-  size_t pin_bytes = 0;
-  struct PinFree { void*& p; ~PinFree() { if (p) cudaFreeHost(p); } } pin_free{pin};
   for (;;) {
     Session* s = nullptr;
     {
@@ -194,25 +188,8 @@ void builder_loop(jfc_server* S) {
     }
     jfc_graph* G = nullptr;
     const Clock::time_point tb = Clock::now();
-    const void* img = s->img.data();
-    const uint8_t* seeds = s->seeds.data();
-    const size_t need = align256(s->img.size()) + s->seeds.size();
-    if (need > pin_bytes) {
-      if (pin) cudaFreeHost(pin);
-      pin = nullptr;
-      pin_bytes = 0;
-      if (cudaMallocHost(&pin, need + need / 4) == cudaSuccess) pin_bytes = need + need / 4;
-      else pin = nullptr;   // no pinned memory: the pageable copies still work
-    }
-    if (pin) {
-      std::memcpy(pin, s->img.data(), s->img.size());
-      std::memcpy((char*)pin + align256(s->img.size()), s->seeds.data(), s->seeds.size());
-      img = pin;
-      seeds = (const uint8_t*)pin + align256(s->img.size());
-    }
     int rc = jfc_graph_create_grid(S->build_ctx, s->dims, s->w, s->h, s->d, s->dims == 2 ? 4 : 6, &G);
-    if (rc == JFC_OK) rc = build_core(G, img, s->pixfmt, seeds, &s->model, cudaMemcpyHostToDevice);
-    cudaStreamSynchronize(S->build_ctx->stream);   // the staging is free again, whatever the outcome
+    if (rc == JFC_OK) rc = build_core(G, s->img.data(), s->pixfmt, s->seeds.data(), &s->model, cudaMemcpyHostToDevice);
     if (S->params.verbose) {
       const Clock::time_point te = Clock::now();
       auto ms = [](Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };

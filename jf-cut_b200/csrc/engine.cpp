@@ -365,7 +365,7 @@ static int finish_bfs(const TileSet& ts, bool cut, const void* pin, int& passes,
   const int* hact = (const int*)((const char*)pin + sizeof(DevCounters));
   passes += hc->bfs_passes;
   if (sweeps_done) *sweeps_done = hc->sweeps_done;
-  if (hc->error) return set_error(JFC_ERR_CUDA, "grid barrier timed out in a persistent kernel");
+  if (hc->error) return set_error(JFC_ERR_CUDA, "a device-side wait timed out in a persistent kernel (grid barrier, worklist or tile staging)");
   if (hc->bfs_status == 2) return set_error(JFC_ERR_NOT_CONVERGED, "BFS pass budget exhausted");
   if (!cut && active) {
     active->resize(ts.ngrids);

@@ -125,7 +125,7 @@ int na_bfs(TileSet& ts, const jfc_params& p, bool cut, cudaStream_t s, int* acti
   DevCounters hc;
   int rc = na_read(&hc, ts.d_ctr, sizeof(hc), s);
   if (rc) return rc;
-  if (hc.error) return set_error(JFC_ERR_CUDA, "grid barrier timed out in a persistent kernel");
+  if (hc.error) return set_error(JFC_ERR_CUDA, "a device-side wait timed out in a persistent kernel (grid barrier, worklist or tile staging)");
   if (hc.bfs_status == 2) return set_error(JFC_ERR_NOT_CONVERGED, "BFS pass budget exhausted");
   if (!cut) {
     rc = na_read(active, ts.d_grid_active, sizeof(int), s);

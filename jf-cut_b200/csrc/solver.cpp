@@ -584,7 +584,7 @@ int jfc_graph_compute_tag(jfc_graph* G, const uint8_t* seeds, uint8_t* tag) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (d_tmp) cudaFreeAsync(d_tmp, s);
   if (e != cudaSuccess) return cuda_status(e, "tag");
-  if (hc.error) return set_error(JFC_ERR_CUDA, "grid barrier timed out in a persistent kernel");
+  if (hc.error) return set_error(JFC_ERR_CUDA, "a device-side wait timed out in a persistent kernel (grid barrier, worklist or tile staging)");
   if (hc.bfs_status == 2) return set_error(JFC_ERR_NOT_CONVERGED, "BFS pass budget exhausted");
   for (size_t i = 0; i < n; ++i) tag[i] = (tag[i] >> 1) & 1u;
   return JFC_OK;

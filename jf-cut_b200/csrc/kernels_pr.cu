@@ -439,9 +439,12 @@ __global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT)
         if (__syncthreads_or(!ok)) {
           if (threadIdx.x == 0) {
             atomicExch(&ctr->error, 1);
-            // copies still in flight land before the CTA leaves (bounded)
-            jfc::mbar_wait(&s_bar[buf], ((parity >> buf) & 1u) ^ 1u, cap);
-            if (pre >= 0) jfc::mbar_wait(&s_bar[pre_buf], (parity >> pre_buf) & 1u, cap);
+            // copies still in flight land before the CTA leaves its shared
+            // memory: bounded by a fixed poll count of its own, not by the
+            // (possibly tiny) spin limit that gave up above
+            constexpr unsigned long long kDrainPolls = 1ull << 26;
+            jfc::mbar_wait(&s_bar[buf], ((parity >> buf) & 1u) ^ 1u, kDrainPolls);
+            if (pre >= 0) jfc::mbar_wait(&s_bar[pre_buf], (parity >> pre_buf) & 1u, kDrainPolls);
           }
           failed = true;
           break;

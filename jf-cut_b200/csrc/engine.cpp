@@ -96,8 +96,10 @@ void tileset_free(TileSet& ts) {
   ts = TileSet();
 }
 
-// Tensor maps of one grid for the push-relabel staging (two CUtensorMap).
-constexpr size_t kTmapBytes = 2 * sizeof(CUtensorMap);
+// Tensor maps of one grid (three CUtensorMap): the push-relabel staging
+// ([0] planes, [1] h with halo) and the 3D relabel frontier's ([1] and [2]
+// the arc-byte plane).
+constexpr size_t kTmapBytes = 3 * sizeof(CUtensorMap);
 // 0: visits load their tiles with ordinary loads (a comparison build)
 #ifndef JFC_PR_TMA
 #define JFC_PR_TMA 1
@@ -120,11 +122,12 @@ static EncodeTiledFn encode_tiled() {
   return fn;
 }
 
-// Encode grid g's staging maps for visits of 32 x ty x tz nodes into out[2]:
+// Encode grid g's staging maps for visits of 32 x ty x tz nodes into out[3]:
 //  [0] the planes {e, h, r[0..K-1]} as one 4D tensor {pitch, Hp, Dp, planes},
 //      box {32, ty, tz, planes};
 //  [1] the h plane {pitch, Hp, Dp}, box {40, ty + 2, tz + 2 (1 in 2D)} (the
-//      tile and its one-cell halo, starting 4 columns left of the tile).
+//      tile and its one-cell halo, starting 4 columns left of the tile);
+//  [2] the arc-byte (label) plane {pitch, Hp, Dp} of bytes, box {32, ty, tz}.
 // Returns false when the planes are not one evenly spaced run or a map is
 // refused; the tile set then stages with ordinary loads.
 static bool encode_pr_maps(const GridDev& g, int ty, int tz, CUtensorMap* out) {
@@ -145,6 +148,12 @@ static bool encode_pr_maps(const GridDev& g, int ty, int tz, CUtensorMap* out) {
     return false;
   const cuuint32_t box3[3] = {40u, (cuuint32_t)(ty + 2), (cuuint32_t)(g.dims == 3 ? tz + 2 : 1)};
   if (fn(&out[1], CU_TENSOR_MAP_DATA_TYPE_INT32, 3, g.h, dims4, str4, box3, unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
+         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  if ((size_t)g.label % 16 || g.pitch % 16) return false;
+  const cuuint64_t strb[2] = {(cuuint64_t)g.pitch, (cuuint64_t)g.pitch * (cuuint64_t)g.Hp};
+  const cuuint32_t boxb[3] = {32u, (cuuint32_t)ty, (cuuint32_t)tz};
+  if (fn(&out[2], CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, g.label, dims4, strb, boxb, unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
   return true;
@@ -280,12 +289,12 @@ int tileset_build(TileSet& ts, int dims, int tile_rows, int tile_depth, const st
   if (s) {
     maps = (CUtensorMap*)((char*)ts.h_stage + o_maps);
   } else {
-    mv.resize(2 * (size_t)ngrids);
+    mv.resize(3 * (size_t)ngrids);
     maps = mv.data();
   }
   bool tma = JFC_PR_TMA && ngrids > 0;
   for (int gi = 0; gi < ngrids && tma; ++gi)
-    tma = encode_pr_maps(grids[gi], ts.pr_split ? 8 : TY, TZ, maps + 2 * gi);
+    tma = encode_pr_maps(grids[gi], ts.pr_split ? 8 : TY, TZ, maps + 3 * gi);
   npar[0] = npar[1] = 0;
   size_t k = 0;
   for (size_t gi = 0; gi < grids.size(); ++gi) {

@@ -96,10 +96,10 @@ struct TileSet {
   int* d_grid_active = nullptr;      // [ngrids] active tiles after global relabel
   unsigned long long* d_pr_ring = nullptr;  // [work items] push-relabel worklist ring (null: sweeps only)
   int* d_pr_lock = nullptr;          // [work items] a visit of the item is in progress
-  const void* d_tmap = nullptr;      // [ngrids][2] tensor maps (128 B each) that stage push-relabel
-                                     // visits: the grid's planes {e, h, r...} with a tile box, and
-                                     // the h plane with a 40-wide tile + halo box (null: visits load
-                                     // their tiles with ordinary loads)
+  const void* d_tmap = nullptr;      // [ngrids][3] tensor maps (128 B each) that stage tile visits:
+                                     // the grid's planes {e, h, r...} with a tile box, the h plane
+                                     // with a 40-wide tile + halo box, the arc-byte plane with a tile
+                                     // box (null: visits load their tiles with ordinary loads)
   void* tmap_slot = nullptr;         // room for d_tmap in the control block
   long long* d_grid_sum = nullptr;   // [ngrids*2] sum min(e,0), source-side count
   DevCounters* d_ctr = nullptr;

@@ -27,6 +27,7 @@
 // word AND/OR.  Reaching a deficit raises cut_bad (the reference's done[1]
 // divergence flag).
 #include "jfc_relax.cuh"
+#include "jfc_tma.cuh"
 
 namespace {
 
@@ -963,10 +964,26 @@ __device__ __forceinline__ void relabel_frontier_warp(const TileSet& ts, int tid
 // costs one closure per turn a shortest path takes instead of one step per
 // level.  Improvements at or above the distance cap are dropped (those
 // nodes stay unreachable).
-template <int DIMS, int TY, int TZ>
+// Staged tile of a 3D frontier visit, filled by two tensor copies: the h
+// plane over the tile and its one-cell halo (40 columns from x0 - 4, as the
+// push-relabel staging) and the tile's arc bytes.
+template <int TY, int TZ>
+struct alignas(128) RlStage {
+  using T = jfc::CtaTile<3, TY, TZ, 40, 4>;
+  static constexpr unsigned kHb = sizeof(int) * T::HN, kLb = 32u * TY * TZ;
+  static constexpr unsigned kBytes = kHb + kLb;   // bytes the two copies deliver
+  int hb[T::HN];
+  alignas(128) uint8_t lb[32 * TY * TZ];
+};
+
+// hb / lb non-null: the tile comes from a staged copy (RlStage) instead of
+// global loads.
+template <int DIMS, int TY, int TZ, bool STAGED = false>
 __device__ __forceinline__ void relabel_frontier_minplus(const TileSet& ts, int tid, int4 ti, const BfsQ& Q,
-                                                         int& cur_grid, int& delta) {
+                                                         int& cur_grid, int& delta, const int* hb = nullptr,
+                                                         const uint8_t* lb = nullptr) {
   constexpr int R = TY * TZ;
+  using ST = jfc::CtaTile<3, TY, TZ, 40, 4>;
   const int lane = threadIdx.x & 31;
   const GridDev& g = ts.d_desc[ti.x];
   const Addr a = make_addr<DIMS, TY, TZ>(g, ti, lane);
@@ -976,9 +993,14 @@ __device__ __forceinline__ void relabel_frontier_minplus(const TileSet& ts, int 
   unsigned posm = 0;
 #pragma unroll
   for (int i = 0; i < R; ++i) {
-    const long long n = roff<TY>(a, i);
-    lab[i] = g.label[n];   // arc byte written by the first pass
-    h0[i] = g.h[n];
+    if constexpr (STAGED) {
+      lab[i] = lb[i * 32 + lane];
+      h0[i] = hb[ST::hidx(lane, i % TY, i / TY)];
+    } else {
+      const long long n = roff<TY>(a, i);
+      lab[i] = g.label[n];   // arc byte written by the first pass
+      h0[i] = g.h[n];
+    }
   }
 #pragma unroll
   for (int i = 0; i < R; ++i) {
@@ -993,23 +1015,34 @@ __device__ __forceinline__ void relabel_frontier_minplus(const TileSet& ts, int 
   int HT[TZ], HB[TZ], HZT[DIMS == 3 ? TY : 1], HZB[DIMS == 3 ? TY : 1];
 #pragma unroll
   for (int z = 0; z < TZ; ++z) {
-    const long long n = roff<TY>(a, z * TY);
-    HT[z] = a.has_yT ? g.h[n - a.pitch] : JFC_INF;
-    HB[z] = a.has_yB ? g.h[n + (long long)TY * a.pitch] : JFC_INF;
+    if constexpr (STAGED) {
+      HT[z] = a.has_yT ? hb[ST::hidx(lane, -1, z)] : JFC_INF;
+      HB[z] = a.has_yB ? hb[ST::hidx(lane, TY, z)] : JFC_INF;
+    } else {
+      const long long n = roff<TY>(a, z * TY);
+      HT[z] = a.has_yT ? g.h[n - a.pitch] : JFC_INF;
+      HB[z] = a.has_yB ? g.h[n + (long long)TY * a.pitch] : JFC_INF;
+    }
   }
   if constexpr (DIMS == 3) {
 #pragma unroll
     for (int y = 0; y < TY; ++y) {
-      const long long n = roff<TY>(a, y);
-      HZT[y] = a.has_zT ? g.h[n - a.slab] : JFC_INF;
-      HZB[y] = a.has_zB ? g.h[n + (long long)TZ * a.slab] : JFC_INF;
+      if constexpr (STAGED) {
+        HZT[y] = a.has_zT ? hb[ST::hidx(lane, y, -1)] : JFC_INF;
+        HZB[y] = a.has_zB ? hb[ST::hidx(lane, y, TZ)] : JFC_INF;
+      } else {
+        const long long n = roff<TY>(a, y);
+        HZT[y] = a.has_zT ? g.h[n - a.slab] : JFC_INF;
+        HZB[y] = a.has_zB ? g.h[n + (long long)TZ * a.slab] : JFC_INF;
+      }
     }
   }
   const int xrow = lane & 15;
   int hx = JFC_INF;
   if (xrow < R && (lane < 16 ? a.has_xL : a.has_xR))
-    hx = g.h[(long long)(lane < 16 ? a.x0 - 1 : a.x0 + 32) + (long long)(a.y0 + xrow % TY) * a.pitch +
-             (long long)(a.z0 + xrow / TY) * a.slab];
+    hx = STAGED ? hb[ST::hidx(lane < 16 ? -1 : 32, xrow % TY, xrow / TY)]
+                : g.h[(long long)(lane < 16 ? a.x0 - 1 : a.x0 + 32) + (long long)(a.y0 + xrow % TY) * a.pitch +
+                  (long long)(a.z0 + xrow / TY) * a.slab];
   // the tile's interior is at its fixpoint (the dense pass or its last
   // visit closed it, and only its own visits write it), so only a halo seed
   // that lowers a border node can change anything
@@ -1149,19 +1182,58 @@ __global__ void __launch_bounds__(256, (DIMS == 3 && TY * TZ > 8) ? 1 : (DIMS ==
 // Warp form of the frontier passes: one warp per queued tile (3D: many
 // tiles per pass, so the visit throughput counts).
 // (level-BFS form: one CTA per SM, its registers; min-plus form: 3 CTAs per
-// SM for 8-row tiles, 2 for 16-row ones, without spills)
+// SM for 8-row tiles, 2 for 16-row ones)
 #ifndef JFC_RELABEL_WARP_MINB
 #define JFC_RELABEL_WARP_MINB 1
 #endif
+#ifndef JFC_RL3D_MINB
+#define JFC_RL3D_MINB 3
+#endif
+// 1: 3D frontier tiles of up to 8 rows are staged by tensor copies
+#ifndef JFC_RL3D_STAGE
+#define JFC_RL3D_STAGE 1
+#endif
 template <int DIMS, int TY, int TZ>
-__global__ void __launch_bounds__(256, JFC_RELABEL_MINPLUS ? (TY * TZ > 8 ? 2 : 3) : JFC_RELABEL_WARP_MINB)
+__global__ void __launch_bounds__(256, JFC_RELABEL_MINPLUS ? (TY * TZ > 8 ? 2 : JFC_RL3D_MINB) : JFC_RELABEL_WARP_MINB)
     k_relabel_warp(TileSet ts, int max_passes) {
   __shared__ int s_items[8][64];   // per-warp staged queue appends (at most 38 before a flush)
   __shared__ int s_cnt[8];
+  // 3D tiles of up to 8 rows with tensor maps: each warp stages its tiles by
+  // tensor copies into two buffers of its own (dynamic shared memory), the
+  // next ticket's tile copied while the current one is visited
+  using Stage = RlStage<TY, TZ>;
+  constexpr bool kStage = JFC_RL3D_STAGE && JFC_RELABEL_MINPLUS && DIMS == 3 && TY * TZ <= 8;
+  __shared__ uint64_t s_bar[8][2];
+  extern __shared__ __align__(128) unsigned char s_dyn[];
   DevCounters* ctr = ts.d_ctr;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool tma = kStage && ts.d_tmap != nullptr;
+  Stage* stage = reinterpret_cast<Stage*>(s_dyn + ((128u - (jfc::smem_addr(s_dyn) & 127u)) & 127u)) + 2 * warp;
   if (lane == 0) s_cnt[warp] = 0;
-  __syncwarp();
+  if (tma && lane == 0) {
+    jfc::mbar_init(&s_bar[warp][0], 1);
+    jfc::mbar_init(&s_bar[warp][1], 1);
+    jfc::fence_mbar_init();
+  }
+  __syncthreads();
+  const unsigned long long spin = jfc::spin_cap(ctr);
+  unsigned parity = 0;      // bit b: phase parity of buffer b's next fill (warp-uniform)
+  int acquired_grid = -1;   // lane 0: grid whose maps it acquired
+  // lane 0: copy tile t4 (grid, tile x / y / z) into buffer b
+  auto issue = [&](int4 t4, int b) {
+    if (lane == 0) {
+      const char* maps = (const char*)ts.d_tmap + (size_t)t4.x * 384;
+      if (t4.x != acquired_grid) {
+        jfc::fence_tmap_acquire(maps + 128);
+        jfc::fence_tmap_acquire(maps + 256);
+        acquired_grid = t4.x;
+      }
+      jfc::fence_async_shared();
+      jfc::mbar_arrive_tx(&s_bar[warp][b], Stage::kBytes);
+      jfc::tma_load_3d(stage[b].hb, maps + 128, t4.y * 32 - 4, t4.z * TY - 1, t4.w * TZ - 1, &s_bar[warp][b]);
+      jfc::tma_load_3d(stage[b].lb, maps + 256, t4.y * 32, t4.z * TY, t4.w * TZ, &s_bar[warp][b]);
+    }
+  };
   unsigned long long visits = 0;
   int cur_grid = -1, delta = 0;
   bool ok = true;
@@ -1199,15 +1271,41 @@ __global__ void __launch_bounds__(256, JFC_RELABEL_MINPLUS ? (TY * TZ > 8 ? 2 : 
       const unsigned kk = k++;
       return (int)kk < n ? queue[kk] : -1;
     };
+    // the previous pass's writes (seen through the grid barrier) come before
+    // this pass's tensor reads
+    if (tma && lane == 0) jfc::fence_async_global();
     int tt = take();
     int4 ti = tt >= 0 ? ts.d_info[tt] : make_int4(0, 0, 0, 0);
+    int buf = 0;
+    if (tma && tt >= 0) issue(ti, buf);
     while (tt >= 0) {
       const int tn = take();
       const int4 tin = tn >= 0 ? ts.d_info[tn] : make_int4(0, 0, 0, 0);
+      if (tma && tn >= 0) issue(tin, buf ^ 1);
       if (lane == 0) fcur[tt] = 0;
       __syncwarp();
-      if (JFC_RELABEL_MINPLUS) relabel_frontier_minplus<DIMS, TY, TZ>(ts, tt, ti, Q, cur_grid, delta);
-      else relabel_frontier_warp<DIMS, TY, TZ>(ts, tt, Q, cur_grid, delta);
+      if (tma) {
+        const unsigned ph = (parity >> buf) & 1u;
+        const bool got = __all_sync(FULL, jfc::mbar_wait(&s_bar[warp][buf], ph, spin));
+        parity ^= 1u << buf;
+        if (!got) {
+          if (lane == 0) {
+            atomicExch(&ctr->error, 1);
+            // copies in flight land before the warp leaves (fixed bound)
+            constexpr unsigned long long kDrainPolls = 1ull << 26;
+            jfc::mbar_wait(&s_bar[warp][buf], ph, kDrainPolls);
+            if (tn >= 0) jfc::mbar_wait(&s_bar[warp][buf ^ 1], (parity >> (buf ^ 1)) & 1u, kDrainPolls);
+          }
+          __syncwarp();
+          break;   // the grid barrier below sees the error: every CTA leaves
+        }
+        relabel_frontier_minplus<DIMS, TY, TZ, true>(ts, tt, ti, Q, cur_grid, delta, stage[buf].hb, stage[buf].lb);
+      } else if (JFC_RELABEL_MINPLUS) {
+        relabel_frontier_minplus<DIMS, TY, TZ>(ts, tt, ti, Q, cur_grid, delta);
+      } else {
+        relabel_frontier_warp<DIMS, TY, TZ>(ts, tt, Q, cur_grid, delta);
+      }
+      buf ^= 1;
       ++visits;
       __syncwarp();
       if (*(volatile int*)Q.scnt >= 32) {
@@ -1514,8 +1612,15 @@ cudaError_t bfs_t(const TileSet& ts, int max_passes, const uint8_t* seeds, cudaS
   else if constexpr (DIMS == 2) fn = (const void*)k_relabel_cta<DIMS, TY, TZ>;
   else fn = (const void*)k_relabel_warp<DIMS, TY, TZ>;
   const int nt = (CUT || DIMS == 3) ? 256 : RTile<DIMS, TY, TZ>::NT;
+  // the 3D frontier's staging buffers: two per warp (dynamic shared memory)
+  const size_t dyn = (!CUT && DIMS == 3 && JFC_RL3D_STAGE && JFC_RELABEL_MINPLUS && TY * TZ <= 8)
+                         ? 2 * 8 * sizeof(RlStage<TY, TZ>) + 128 : 0;
+  if (dyn > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e != cudaSuccess) return e;
+  }
   static int cache[64] = {0};
-  const int blocks = persistent_blocks_cached(cache, fn, nt);
+  const int blocks = persistent_blocks_cached(cache, fn, nt, dyn);
   if (!CUT) {
     const long long fb = ((long long)ts.ntiles * 32 + 255) / 256;
     jfc_note_launch();
@@ -1526,7 +1631,7 @@ cudaError_t bfs_t(const TileSet& ts, int max_passes, const uint8_t* seeds, cudaS
   TileSet arg = ts;
   void* params[] = {(void*)&arg, (void*)&max_passes, (void*)&seeds};   // relabel kernels take two
   jfc_note_launch();
-  return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(nt), params, 0, s);
+  return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(nt), params, dyn, s);
 }
 
 template <int TY, int TZ>

@@ -120,7 +120,7 @@ template <int DIMS, int TY, int TZ, bool SPLIT>
 __device__ __forceinline__ void pr_stage_issue(const TileSet& ts, int tid, PrStage<DIMS, TY, TZ>& st, uint64_t* bar,
                                                int& acquired_grid) {
   const int4 o = item_origin<DIMS, TY, TZ, SPLIT>(ts, tid);
-  const char* maps = (const char*)ts.d_tmap + (size_t)o.x * 256;
+  const char* maps = (const char*)ts.d_tmap + (size_t)o.x * 384;   // three maps per grid
   if (o.x != acquired_grid) {
     jfc::fence_tmap_acquire(maps);
     jfc::fence_tmap_acquire(maps + 128);

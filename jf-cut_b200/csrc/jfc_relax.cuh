@@ -49,40 +49,30 @@ struct CtaTile {
 // Arc bits used by the relaxation: bit 0 +x, 1 +y, 2 -y, 3 -x, 4 +z, 5 -z.
 constexpr unsigned A_XP = 1u, A_YP = 2u, A_YM = 4u, A_XM = 8u, A_ZP = 16u, A_ZM = 32u;
 
-// One line of L nodes handled by L lanes (shuffle width L): min-plus closure
-// h(p) = min(h(p), h(p+k) + k) along residual arcs towards +d (bit fwd), then
-// towards -d (bit bwd), by shuffle doubling; the halo values at both ends are
-// folded into the end lanes first.
+// One line of L nodes handled by L lanes (shuffle width L, lane p of its
+// segment): min-plus closure h(p) = min(h(p), h(p+k) + k) along runs of
+// residual arcs towards +d (bit fwd), then towards -d (bit bwd), by shuffle
+// doubling; the halo values at both ends are folded into the end lanes
+// first.  The arc runs come from two warp ballots of the arc bits (bits p ..
+// p+k-1 of the segment set), so only the values move between lanes.
 template <int L>
 __device__ __forceinline__ bool line_scan(int* h, int i, int stride, unsigned a, int p, unsigned fwd,
                                           unsigned bwd) {
+  const int lane = threadIdx.x & 31;
+  const unsigned fm = __ballot_sync(FULL, (a & fwd) != 0u), bm = __ballot_sync(FULL, (a & bwd) != 0u);
   const int v = h[i];
   int vv = v;
   if (p == L - 1 && (a & fwd)) vv = min(vv, h[i + stride] + 1);
-  bool o = (a & fwd) != 0;
 #pragma unroll
   for (int off = 1; off < L; off <<= 1) {
     const int nv = __shfl_down_sync(FULL, vv, off, L);
-    const int no = __shfl_down_sync(FULL, (int)o, off, L);
-    if (p + off < L) {
-      if (o) vv = min(vv, nv + off);
-      o = o && no;
-    } else {
-      o = false;
-    }
+    if (p + off < L && ((~fm >> lane) & ((1u << off) - 1u)) == 0u) vv = min(vv, nv + off);
   }
   if (p == 0 && (a & bwd)) vv = min(vv, h[i - stride] + 1);
-  o = (a & bwd) != 0;
 #pragma unroll
   for (int off = 1; off < L; off <<= 1) {
     const int nv = __shfl_up_sync(FULL, vv, off, L);
-    const int no = __shfl_up_sync(FULL, (int)o, off, L);
-    if (p >= off) {
-      if (o) vv = min(vv, nv + off);
-      o = o && no;
-    } else {
-      o = false;
-    }
+    if (p >= off && ((~bm >> (lane - off + 1)) & ((1u << off) - 1u)) == 0u) vv = min(vv, nv + off);
   }
   if (vv < v) {
     h[i] = vv;

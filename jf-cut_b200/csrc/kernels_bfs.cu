@@ -1396,8 +1396,13 @@ __device__ __forceinline__ bool border_improvable(const TileSet& ts, int tid, in
   return __any_sync(jfc::FULL, imp);
 }
 
+// (32 x 8 tiles: 6 CTAs per SM, the worklist's pollers and the border check's warps)
+#ifndef JFC_RL2D_MINB
+#define JFC_RL2D_MINB 6
+#endif
 template <int DIMS, int TY, int TZ>
-__global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT) k_relabel_cta(TileSet ts, int max_passes) {
+__global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT, (DIMS == 2 && TY == 8) ? JFC_RL2D_MINB : 1)
+    k_relabel_cta(TileSet ts, int max_passes) {
   __shared__ RlSmem<DIMS, TY, TZ> sm;
   DevCounters* ctr = ts.d_ctr;
   const int lane = threadIdx.x & 31;

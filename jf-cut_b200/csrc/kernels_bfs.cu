@@ -1401,7 +1401,8 @@ __device__ __forceinline__ bool border_improvable(const TileSet& ts, int tid, in
 #define JFC_RL2D_MINB 6
 #endif
 template <int DIMS, int TY, int TZ>
-__global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT, (DIMS == 2 && TY == 8) ? JFC_RL2D_MINB : 1)
+__global__ void __launch_bounds__(RTile<DIMS, TY, TZ>::NT,
+                                  (DIMS == 2 && TY == 8) ? JFC_RL2D_MINB : RTile<DIMS, TY, TZ>::NT > 256 ? 2 : 3)
     k_relabel_cta(TileSet ts, int max_passes) {
   __shared__ RlSmem<DIMS, TY, TZ> sm;
   DevCounters* ctr = ts.d_ctr;

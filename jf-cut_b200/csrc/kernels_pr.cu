@@ -363,12 +363,14 @@ __device__ __forceinline__ int pr_visit(const TileSet& ts, int tid, int local_it
 // a second ticket would only keep another CTA idle).  A prefetched item is
 // safe to read early: items of one sweep are never adjacent, so nothing
 // writes its tile or its halo heights until the sweep ends.
-// CTAs per SM the 2D 32 x 8 phase is compiled for (its registers)
+// CTAs per SM the phase is compiled for (its registers): the 2D 32 x 8 form
+// JFC_PR2D_MINB, other 256-node tiles 3, 512-node tiles 2
 #ifndef JFC_PR2D_MINB
 #define JFC_PR2D_MINB 4
 #endif
 template <int DIMS, int TY, int TZ, bool SPLIT>
-__global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT, (DIMS == 2 && TY == 8) ? JFC_PR2D_MINB : 1)
+__global__ void __launch_bounds__(Tile<DIMS, TY, TZ>::NT,
+                                  (DIMS == 2 && TY == 8) ? JFC_PR2D_MINB : Tile<DIMS, TY, TZ>::NT > 256 ? 2 : 3)
     k_pr_phase(TileSet ts, int sweeps, int local_iters) {
   using Stage = PrStage<DIMS, TY, TZ>;
   __shared__ PrSmem<DIMS, TY, TZ> sm;

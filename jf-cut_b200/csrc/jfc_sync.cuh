@@ -55,8 +55,10 @@ __device__ __forceinline__ int vload(const int* p) { return *(const volatile int
 
 // Distance cap of the running global relabel: distances at or above it are
 // stored as unreachable (JFC_INF); no cap when ctr->h_cap is 0.
+// (set before the kernel that reads it runs, constant during it: an ordinary
+// cached load, not a poll of L2 on every tile visit)
 __device__ __forceinline__ int height_cap(const DevCounters* ctr) {
-  const int v = vload(&ctr->h_cap);
+  const int v = ctr->h_cap;
   return v > 0 ? v : JFC_INF;
 }
 // The cap for grid g: its own when set, else the tile set's.

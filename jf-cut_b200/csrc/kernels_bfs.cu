@@ -490,6 +490,9 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
   // heights other CTAs write while the worklist runs are read from L2 (the
   // SM's L1 may hold an older copy of the line)
   const bool fresh = W.ring != nullptr;
+  // (thread 0) the tile's activity byte as its last visit left it, read early
+  unsigned act_old = 0;
+  if (t == 0) act_old = fresh ? __ldcg(ts.d_act + tid) : ts.d_act[tid];
   const int hstart = fresh ? __ldcg(g.h + n) : g.h[n];
   s.h[hi] = hstart;
   for (int c = t; c < T::NHALO; c += T::NT) {
@@ -567,7 +570,7 @@ __device__ __forceinline__ void relabel_visit(const TileSet& ts, int tid, RlSmem
       jfc::warp_append(want, nb, Q.flags, Q.q, Q.qn);
     }
     if (t == 0) {
-      const int old = ((fresh ? __ldcg(ts.d_act + tid) : ts.d_act[tid]) & 3u) != 0 ? 1 : 0;
+      const int old = (act_old & 3u) != 0 ? 1 : 0;
       ts.d_act[tid] = (uint8_t)((act_lo ? 1 : 0) | (act_hi ? 2 : 0));
       if (ti.x != cur_grid) {
         if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
@@ -943,7 +946,7 @@ __device__ __forceinline__ void relabel_frontier_warp(const TileSet& ts, int tid
   act_hi = __any_sync(FULL, act_hi);
   const bool act = act_lo || act_hi;
   if (lane == 0) {
-    const int old = (ts.d_act[tid] & 3u) != 0 ? 1 : 0;
+    const int old = (__ldcg(ts.d_act + tid) & 3u) != 0 ? 1 : 0;
     ts.d_act[tid] = (uint8_t)((act_lo ? 1 : 0) | (act_hi ? 2 : 0));
     if (ti.x != cur_grid) {
       if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
@@ -987,6 +990,10 @@ __device__ __forceinline__ void relabel_frontier_minplus(const TileSet& ts, int 
   const int lane = threadIdx.x & 31;
   const GridDev& g = ts.d_desc[ti.x];
   const Addr a = make_addr<DIMS, TY, TZ>(g, ti, lane);
+  // the tile's activity byte as the last visit left it (another SM's write of
+  // an earlier pass: read from L2, and early, so its latency overlaps the
+  // closure)
+  const unsigned act_old = lane == 0 ? (unsigned)__ldcg(ts.d_act + tid) : 0u;
   unsigned lab[R];
   int hv[R], h0[R];
   unsigned AXP[R], AXM[R];
@@ -1095,7 +1102,7 @@ __device__ __forceinline__ void relabel_frontier_minplus(const TileSet& ts, int 
   act_hi = __any_sync(FULL, act_hi);
   const bool act = act_lo || act_hi;
   if (lane == 0) {
-    const int old = (ts.d_act[tid] & 3u) != 0 ? 1 : 0;
+    const int old = (act_old & 3u) != 0 ? 1 : 0;
     ts.d_act[tid] = (uint8_t)((act_lo ? 1 : 0) | (act_hi ? 2 : 0));
     if (ti.x != cur_grid) {
       if (delta && cur_grid >= 0) atomicAdd(&ts.d_grid_active[cur_grid], delta);
@@ -1263,7 +1270,9 @@ __global__ void __launch_bounds__(256, JFC_RELABEL_MINPLUS ? (TY * TZ > 8 ? 2 : 
     auto take = [&]() -> int {
       if (k >= kend) {
         unsigned v = 0;
-        const unsigned c = jfc::vload((const int*)&ctr->ticket[cb]) + round * kChunk < (unsigned)n ? kChunk : 1u;
+        // chunk size from the warp's last ticket (a lower bound on the
+        // counter): no extra read of the counter on the way to its update
+        const unsigned c = (long long)k + round * kChunk < n ? kChunk : 1u;
         if (lane == 0) v = atomicAdd(&ctr->ticket[cb], c);
         k = __shfl_sync(FULL, v, 0);
         kend = k + c;

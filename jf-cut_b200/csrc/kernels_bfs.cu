@@ -1188,13 +1188,15 @@ __global__ void __launch_bounds__(256, (DIMS == 3 && TY * TZ > 8) ? 1 : (DIMS ==
 // graphcut_count_block.cl:19-65, as one warp-aggregated append).
 // Warp form of the frontier passes: one warp per queued tile (3D: many
 // tiles per pass, so the visit throughput counts).
-// (level-BFS form: one CTA per SM, its registers; min-plus form: 3 CTAs per
-// SM for 8-row tiles, 2 for 16-row ones)
+// (level-BFS form: one CTA per SM, its registers; min-plus form: 2 CTAs per
+// SM, the registers the two-ahead ticket pipeline holds without spills: 3
+// CTAs per SM spilled and measured slower, 116.5 vs 104-108.5 ms of frontier
+// per video solve)
 #ifndef JFC_RELABEL_WARP_MINB
 #define JFC_RELABEL_WARP_MINB 1
 #endif
 #ifndef JFC_RL3D_MINB
-#define JFC_RL3D_MINB 3
+#define JFC_RL3D_MINB 2
 #endif
 // 1: 3D frontier tiles of up to 8 rows are staged by tensor copies
 #ifndef JFC_RL3D_STAGE
@@ -1283,14 +1285,20 @@ __global__ void __launch_bounds__(256, JFC_RELABEL_MINPLUS ? (TY * TZ > 8 ? 2 : 
     // the previous pass's writes (seen through the grid barrier) come before
     // this pass's tensor reads
     if (tma && lane == 0) jfc::fence_async_global();
+    // Two tickets ahead: the current tile tt is staged in `buf`, the next
+    // one tn is being copied into the other buffer, and the ticket and tile
+    // of the one after (tnn) are fetched while tt is visited; tnn's copy goes
+    // into `buf` once tt's visit has read it.
     int tt = take();
     int4 ti = tt >= 0 ? ts.d_info[tt] : make_int4(0, 0, 0, 0);
     int buf = 0;
     if (tma && tt >= 0) issue(ti, buf);
+    int tn = tt >= 0 ? take() : -1;
+    int4 tin = tn >= 0 ? ts.d_info[tn] : make_int4(0, 0, 0, 0);
+    if (tma && tn >= 0) issue(tin, buf ^ 1);
     while (tt >= 0) {
-      const int tn = take();
-      const int4 tin = tn >= 0 ? ts.d_info[tn] : make_int4(0, 0, 0, 0);
-      if (tma && tn >= 0) issue(tin, buf ^ 1);
+      const int tnn = tn >= 0 ? take() : -1;
+      const int4 tinn = tnn >= 0 ? ts.d_info[tnn] : make_int4(0, 0, 0, 0);
       if (lane == 0) fcur[tt] = 0;
       __syncwarp();
       if (tma) {
@@ -1309,6 +1317,8 @@ __global__ void __launch_bounds__(256, JFC_RELABEL_MINPLUS ? (TY * TZ > 8 ? 2 : 
           break;   // the grid barrier below sees the error: every CTA leaves
         }
         relabel_frontier_minplus<DIMS, TY, TZ, true>(ts, tt, ti, Q, cur_grid, delta, stage[buf].hb, stage[buf].lb);
+        __syncwarp();   // every lane has read `buf` before it is refilled
+        if (tnn >= 0) issue(tinn, buf);
       } else if (JFC_RELABEL_MINPLUS) {
         relabel_frontier_minplus<DIMS, TY, TZ>(ts, tt, ti, Q, cur_grid, delta);
       } else {
@@ -1325,6 +1335,8 @@ __global__ void __launch_bounds__(256, JFC_RELABEL_MINPLUS ? (TY * TZ > 8 ? 2 : 
       }
       tt = tn;
       ti = tin;
+      tn = tnn;
+      tin = tinn;
     }
     __syncwarp();
     flush_staged(Q, lane);

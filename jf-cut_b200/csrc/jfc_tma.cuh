@@ -1,6 +1,7 @@
 // jfc_tma.cuh — tensor-memory-access (TMA) staging helpers for sm_100a:
 // shared-memory mbarriers, tiled bulk tensor loads from this GPU's own global
-// memory (no cluster multicast), and the proxy fences they need.
+// memory into the issuing CTA's own shared memory, and the proxy fences they
+// need.
 #pragma once
 
 #include <cstdint>

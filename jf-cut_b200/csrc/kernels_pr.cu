@@ -687,7 +687,9 @@ cudaError_t launch_t(const TileSet& ts, int sweeps, int local_iters, cudaStream_
   // visited, one being filled), one for the worklist; + 128 B to align them
   const size_t dyn = sizeof(PrStage<DIMS, TY, TZ>) * (async ? 1 : 2) + 128;
   static int cache_sweeps[64] = {0}, cache_async[64] = {0};
-  if (dyn > 48 * 1024) {
+  // without this opt-in a kernel's dynamic shared memory is limited to 48 KB
+  // minus its static shared memory
+  {
     const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
   }

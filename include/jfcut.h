@@ -106,8 +106,9 @@ typedef struct jfc_params {
                             1 = checkerboard parity sweeps with a grid barrier between colours,
                             2 = an asynchronous worklist with per-tile neighbour exclusion (no
                             barriers), 3 = sweeps while more than 1/256 of the tiles are active
-                            and the worklist in the tail, 0 = automatic.  Same arithmetic, same
-                            results */
+                            and the worklist in the tail, 0 = automatic (sweeps, and the worklist
+                            for the cycles after the exact relabel of relabel_cap when it finds
+                            excess left).  Same arithmetic, same results */
   int local_iters_tail;  /* push/relabel rounds per visit once fewer than 1/256 of the tiles are
                             active (the long-path tail of a solve, where excess has to cross
                             whole tiles): 0 = automatic, < 0 = local_iters */

@@ -578,6 +578,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   bool graphs = false;
   double fast_ms = 0.0;   // Fast-Cut iterations (event-timed: many small launches)
   unsigned long long last_pr = 0, last_gr = 0;
+  bool post_exact = false;   // the exact relabel ran and found reachable excess
   {
     const DevCounters* c0 = (const DevCounters*)ctx->h_pin;
     last_pr = c0->ns_pr;
@@ -610,8 +611,12 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
       // excess crosses a whole tile per visit instead of per several sweeps
       const bool tail = total() * 256 < (long long)ts.ntiles;
       const int li = tail ? tail_iters : p.local_iters;
-      // pr_sched 3: parity sweeps in the bulk, the worklist in the tail
-      const int sched = pr_sched_for(p) == 3 ? (tail ? 2 : 1) : pr_sched_for(p);
+      // pr_sched 3: parity sweeps in the bulk, the worklist in the tail;
+      // automatic: the worklist once the exact relabel found excess farther
+      // than the cap from every deficit (a few tiles whose excess crosses
+      // many tiles, where the sweeps would idle at their barriers)
+      const int sched = pr_sched_for(p) == 3 ? (tail ? 2 : 1) : (p.pr_sched == 0 && post_exact) ? 2
+                                                                                               : pr_sched_for(p);
       rc = run_cycle(ctx, ts, p, interval, h_cap, li, sched, st.bfs_passes, active, &sw, &graphs);
       last_cap = h_cap;
       ++st.pr_phases;
@@ -656,6 +661,7 @@ int engine_solve(jfc_ctx* ctx, TileSet& ts, const jfc_params& p_in, std::vector<
   if (p.verbose)
     fprintf(stderr, "{\"relabel\": %d, \"exact\": true, \"active_tiles\": %lld}\n", st.global_relabels, total());
   if (total() == 0) break;
+  post_exact = true;
   }
   if (status != JFC_OK) {
     for (int g = 0; g < ts.ngrids; ++g)

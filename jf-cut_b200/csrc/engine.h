@@ -84,8 +84,8 @@ inline int interval_for(const jfc_params& p, int dims) {
   return p.relabel_interval > 0 ? p.relabel_interval : (dims == 2 ? 2 : 3);
 }
 // Push-relabel visit scheduling (1 sweeps, 2 worklist, 3 sweeps while many
-// tiles are active and the worklist in the tail): pr_sched, or the measured
-// default when it is 0.
+// tiles are active and the worklist in the tail): pr_sched, or the sweeps when
+// it is 0 (engine_solve then switches to the worklist after the exact relabel).
 inline int pr_sched_for(const jfc_params& p) { return p.pr_sched >= 1 && p.pr_sched <= 3 ? p.pr_sched : 1; }
 // Distance cap of the global relabels while solving (0: none): relabel_cap,
 // or when it is 0 the measured default per dimensionality.  The Fast-Cut

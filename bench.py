@@ -696,7 +696,8 @@ def main():
                                      if pr_traffic_per_visit() else None),
                          "algorithmic_bytes_per_launch": visits * bytes_per_visit / max(1, pr_launches),
                          "launches": pr_launches,
-                         "kernel": "k_pr_phase (push-relabel phases; %d B per tile visit algorithmic, %s peak; "
+                         "kernel": "k_pr_phase / k_pr_async (push-relabel phases: parity sweeps, and the "
+                                   "worklist after the exact relabel; %d B per tile visit algorithmic, %s peak; "
                                    "traffic: DRAM bytes per visit of the committed one-pass ncu capture of "
                                    "this workload's push-relabel launches times the visits per launch)"
                                    % (bytes_per_visit, peak_kind)},
